@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Benchmark: atoms/s for SOAP + dP/dr on one B200.
+
+Workload (the single-structure GPU configuration): non-periodic (H2O)_1000
+cluster, 3000 atoms on a jittered 10x10x10 lattice (seeded, synthetic);
+species H, O; r_cut 10, n_max 7, l_max 3, sigma 0.5, gto, average off.
+One step = the descriptor plus the analytical dP/dr of every centre w.r.t.
+every atom, (3000, 3000, 3, 420) float32 = 45.4 GB, through the public API
+``SOAP.derivatives`` (the same call as the reference's examples).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints ONE JSON line.  ``value`` is device-resident throughput (inputs in
+HBM, CUDA events around every step, max over ranks); ``e2e`` is the same
+call with the positions copied from pinned host memory and both outputs
+copied back to pinned host memory inside the timed region; ``roofline`` is
+the Jacobian kernel (an HBM write stream) timed with CUDA events during the
+timed steps; ``cpu_baseline`` is the FP64 oracle restatement of the
+reference's CPU path on a bounded sample.  Under torchrun each rank runs its
+own copy of the workload (weak scaling, no data-path collective).
+``--impl reference`` times the reference's CPU algorithm (the oracle port;
+the reference itself is Python and does not travel) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atoms/s for SOAP + dP/dr, fused batched vs plain, 1 B200, rel err <= 1e-5"
+UNIT = "atoms/s"
+WORKLOAD = "cluster3000"
+CONFIG = {
+    "workload": "(H2O)_1000 non-periodic water cluster, 3000 atoms; species H,O; r_cut=10, n_max=7, l_max=3, "
+                "sigma=0.5, gto, average=off; create + analytical dP/dr (3000 x 3000 x 3 x 420 float32)",
+    "atoms_per_step": 3000,
+    "features": 420,
+    "l2": "each step writes 45.4 GB (> 126 MB L2); L2 also flushed between timed steps",
+}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _traffic_from_profiles():
+    """Per-launch DRAM bytes of the Jacobian kernel at this workload, from the
+    committed ncu summary (None when absent)."""
+    path = os.path.join(ROOT, "profiles", "jacobian_cluster3000.md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("traffic_bytes_per_launch_full:"):
+                return float(line.split(":", 1)[1].strip().split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_sample(n_centres: int = 24, workers: int = 1):
+    """Oracle (FP64 numpy restatement of the reference path) on a bounded
+    sample: create over all 3000 centres plus the dense Jacobian of
+    n_centres centres; scaled to atoms/s of the full step."""
+    from oracle.soap_oracle import OracleSOAP
+    from cusoap_b200 import workloads as W
+    sysd = W.make(WORKLOAD)
+    o = OracleSOAP(**W.CONFIGS[WORKLOAD])
+    pos, Z = sysd["positions"], sysd["atomic_numbers"]
+    t0 = time.perf_counter()
+    o.create(pos, Z)
+    t_create = time.perf_counter() - t0
+    rng = np.random.default_rng(0)
+    cen = [int(c) for c in rng.choice(3000, n_centres, replace=False)]
+    t0 = time.perf_counter()
+    o.derivatives(pos, Z, centers=cen, return_descriptor=False)
+    t_der = time.perf_counter() - t0
+    per_atom = t_create / 3000 + t_der / n_centres
+    return {"value": 1.0 / per_atom, "unit": UNIT, "cores": workers, "kind": "port",
+            "sample": f"oracle create of all 3000 centres ({t_create:.2f} s) + dense FP64 Jacobian of "
+                      f"{n_centres} sampled centres ({t_der:.2f} s), scaled to one full step",
+            "seconds": t_create + t_der}
+
+
+def _ref_worker(args):
+    kind, centres = args
+    from oracle.soap_oracle import OracleSOAP
+    from cusoap_b200 import workloads as W
+    sysd = W.make(WORKLOAD)
+    o = OracleSOAP(**W.CONFIGS[WORKLOAD])
+    t0 = time.perf_counter()
+    if kind == "create":
+        o.create(sysd["positions"], sysd["atomic_numbers"], centers=centres)
+    else:
+        o.derivatives(sysd["positions"], sysd["atomic_numbers"], centers=centres, return_descriptor=False)
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU algorithm (oracle port) on all
+    host cores, one bounded sample per step."""
+    import multiprocessing as mp
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    workers = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    rng = np.random.default_rng(1)
+    per_step = []
+    with ctx.Pool(workers) as pool:
+        def one_step():
+            chunks = np.array_split(np.arange(3000), workers)
+            dcen = [int(c) for c in rng.choice(3000, 2 * workers, replace=False)]
+            t0 = time.perf_counter()
+            pool.map(_ref_worker, [("create", [int(x) for x in ch]) for ch in chunks])
+            t_create = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            pool.map(_ref_worker, [("deriv", dcen[k::workers]) for k in range(workers)])
+            t_der = time.perf_counter() - t0
+            # the sampled Jacobian rows scale linearly with the centre count
+            return t_create + t_der * 3000 / len(dcen)
+        for _ in range(max(1, args.warmup)):
+            one_step()
+        for _ in range(args.steps):
+            per_step.append(one_step())
+    t = sum(per_step) / len(per_step)
+    value = 3000.0 / t
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": dict(CONFIG, parallelism="host cores"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+                             "sample": f"per step: oracle create of all 3000 centres + dense FP64 Jacobian of "
+                                       f"{2 * workers} sampled centres, scaled to 3000 centres; {workers} "
+                                       f"spawned worker processes"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def batched_vs_plain(soap_cls, torch):
+    """The batched workload with forces: 512 periodic cells of 8-400 atoms
+    (n_max 8, l_max 6, 4 species), descriptor + adjoint forces of
+    E = sum w.p, one batched launch per stage vs a per-structure loop."""
+    from cusoap_b200 import workloads as W
+    cells = W.make("cells512")
+    soap = soap_cls(**W.CONFIGS["cells512"])
+    rng = np.random.default_rng(0)
+    w = torch.tensor(rng.standard_normal(soap.get_number_of_features()), dtype=torch.float32, device="cuda")
+    dev_cells = [{"positions": torch.tensor(c["positions"], device="cuda"), "atomic_numbers": c["atomic_numbers"],
+                  "cell": c["cell"], "pbc": c["pbc"]} for c in cells]
+    n_atoms = sum(len(c["atomic_numbers"]) for c in cells)
+
+    def batched():
+        sysl = []
+        for c in dev_cells:
+            d = dict(c)
+            d["positions"] = c["positions"].clone().requires_grad_(True)
+            sysl.append(d)
+        out = soap.create(sysl)
+        E = sum((o * w).sum() for o in out) if isinstance(out, list) else (out * w).sum()
+        E.backward()
+        return sysl
+
+    def plain():
+        for c in dev_cells:
+            d = dict(c)
+            d["positions"] = c["positions"].clone().requires_grad_(True)
+            (soap.create(d) * w).sum().backward()
+
+    res = {}
+    for name, fn in (("batched", batched), ("plain", plain)):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 3
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        res[name] = n_atoms * reps / (e0.elapsed_time(e1) / 1e3)
+    return {"workload": "512 periodic cubic cells, 8-400 atoms (104k atoms), 4 species, r_cut 6, n_max 8, l_max 6, "
+                        "sigma 0.4; descriptor + adjoint forces of E = sum w.p per step",
+            "batched_atoms_per_s": res["batched"], "plain_atoms_per_s": res["plain"],
+            "speedup": res["batched"] / res["plain"]}
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = _dist()
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    device = torch.device("cuda", torch.cuda.current_device())
+    from cusoap_b200 import SOAP, _lib, workloads as W
+    sysd = W.make(WORKLOAD) if args.nx == 10 else W.water_cluster(args.nx, args.nx, args.nx, seed=0)
+    n_at = len(sysd["atomic_numbers"])
+    soap = SOAP(**W.CONFIGS[WORKLOAD], device=device)
+    pos_d = torch.tensor(sysd["positions"], dtype=torch.float64, device=device)
+    Z = sysd["atomic_numbers"]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+
+    def step():
+        return soap.derivatives({"positions": pos_d, "atomic_numbers": Z}, return_descriptor=True)
+
+    for _ in range(args.warmup):
+        J, D = step()
+        del J, D
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timed region ----
+    clocks = Clocks(torch.cuda.current_device() if world == 1 else local)
+    soap.profile = []
+    launches0 = _lib.kernel_launches()
+    evs = []
+    barrier()
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        J, D = step()
+        e1.record()
+        evs.append((e0, e1))
+        del J, D
+    barrier()
+    launches = _lib.kernel_launches() - launches0
+    clk = clocks.stop()
+    stage = soap.stage_times()
+    soap.profile = None
+    t_ms = sum(a.elapsed_time(b) for a, b in evs)
+    if world > 1:
+        tt = torch.tensor([t_ms], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    ms_per_step = t_ms / args.steps
+    value = world * float(n_at) * args.steps / (t_ms / 1e3)
+
+    # ---- roofline of the Jacobian kernel (HBM write stream) ----
+    jac_ms = stage.get("jacobian", float("nan")) / args.steps
+    jac_bytes = n_at * n_at * 3 * 420 * 4
+    peak, peak_kind = _peaks()
+    achieved = jac_bytes / (jac_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": _traffic_from_profiles(), "kernel": "k_jacobian<3>",
+                "peak_kind": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6.65 TB/s",
+                "algorithmic_bytes_per_launch": jac_bytes, "ms_per_launch": jac_ms,
+                "stage_ms_per_step": {k: v / args.steps for k, v in stage.items()}}
+
+    # ---- end to end: pinned host in, pinned host out ----
+    e2e = None
+    if not args.no_e2e:
+        pos_h = torch.tensor(sysd["positions"], dtype=torch.float64).pin_memory()
+        J_h = torch.empty((n_at, n_at, 3, 420), dtype=torch.float32, pin_memory=True)
+        D_h = torch.empty((n_at, 420), dtype=torch.float32, pin_memory=True)
+        n_e2e = max(1, min(args.steps, args.e2e_steps))
+
+        def e2e_step():
+            p = pos_h.to(device, non_blocking=True)
+            J, D = soap.derivatives({"positions": p, "atomic_numbers": Z}, return_descriptor=True)
+            J_h.copy_(J, non_blocking=True)
+            D_h.copy_(D, non_blocking=True)
+            del J, D
+
+        e2e_step()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n_e2e):
+            e2e_step()
+        e1.record()
+        barrier()
+        te = e0.elapsed_time(e1)
+        if world > 1:
+            tt = torch.tensor([te], dtype=torch.float64, device=device)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            te = float(tt.item())
+        e2e = {"value": world * float(n_at) * n_e2e / (te / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(pos_h.numel() * 8 + n_at * 4),
+               "d2h_bytes_per_step": int(J_h.numel() * 4 + D_h.numel() * 4), "steps": n_e2e,
+               "note": "positions from pinned host; descriptor and full Jacobian copied back to pinned host"}
+        del J_h, D_h
+
+    extra = None
+    if not args.no_batched and rank == 0:
+        try:
+            extra = batched_vs_plain(SOAP, torch)
+        except Exception as exc:  # reported, never silently dropped
+            extra = {"error": repr(exc)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu and args.nx == 10:
+        cpu = cpu_baseline_sample()
+
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": dict(CONFIG, parallelism=f"replicas x{world}" if world > 1 else "single GPU")
+            if args.nx == 10 else {"workload": f"profiling case: {n_at}-atom water cluster, same parameters"},
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk, "cpu_baseline": cpu,
+            "batched_vs_plain": extra}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--nx", type=int, default=10, help="lattice edge of the water cluster (10 = the workload; "
+                                                         "smaller only for profiling captures)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

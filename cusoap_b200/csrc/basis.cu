@@ -1,0 +1,296 @@
+// GTO basis, Loewdin orthonormalisation and FP32 radial tables, built once
+// per basis in FP64 on the device.
+//
+// Reference: SOAP._init_gto_basis (soap_generator.py:690-708),
+// _lowdin_invsqrt (:339-343), the cutoff padding (:600-602), the radial
+// factors of the closed-form derivative (:2389-2402) and the feature slices
+// (:1215-1291).
+//
+// The Loewdin matrices beta_l = S_l^{-1/2} have entries up to ~1e3 with
+// heavy cancellation (overlap condition numbers ~1e6 at n_max = 8), so the
+// orthonormal radial functions
+//     B_nl(r)    = sum_k beta^l_nk pref_kl exp(-gamma_kl r^2)
+//     Bhat_nl(r) = sum_k beta^l_nk (-2 gamma_kl) pref_kl exp(-gamma_kl r^2)
+// cannot be evaluated to 1e-6 from FP32 exponentials.  Instead they are
+// sampled here in FP64 and stored as degree-7 polynomials on uniform radial
+// segments (Chebyshev interpolation, converted to monomials in the local
+// coordinate t in [-1, 1]); the kernels evaluate them with 7 FP32 FMAs.  The
+// build measures the table error against the FP64 functions and stores it.
+#include <math.h>
+
+#include "common.cuh"
+
+namespace soapb {
+
+struct BasisDev {
+  int N, L, S, crossover, nseg, F;
+  double r_cut, eta, cutoff, h;
+  double* alpha;
+  double* beta;
+  float* tab_b;
+  float* tab_bh;
+  int* ftab;
+  double* err;
+};
+
+__device__ void atomic_max_nonneg(double* addr, double v) {
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+__global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
+  const int N = a.N, L = a.L, NF = N * (L + 1);
+  __shared__ double s_gamma[(kMaxL + 1) * kMaxN];
+  __shared__ double s_pref[(kMaxL + 1) * kMaxN];
+  __shared__ int s_boff[kMaxS * kMaxS * (kMaxL + 1)];
+  const int tid = threadIdx.x;
+
+  // alpha_{l,n} = -ln(1e-3 / a_n^l) / a_n^2, a = linspace(1, r_cut, N)
+  for (int i = tid; i < NF; i += blockDim.x) {
+    const int l = i / N, n = i % N;
+    const double an = (N == 1) ? 1.0 : 1.0 + (a.r_cut - 1.0) * (double)n / (double)(N - 1);
+    const double al = -log(1e-3 / pow(an, (double)l)) / (an * an);
+    a.alpha[l * N + n] = al;
+    const double p = al + a.eta;
+    s_gamma[l * kMaxN + n] = al * a.eta / p;
+    s_pref[l * kMaxN + n] = pow(kPi, 1.5) * pow(a.eta / p, (double)l) * pow(p, -1.5);
+  }
+  __syncthreads();
+
+  // S_l, Jacobi eigendecomposition, beta_l = V diag(clamp(w, 1e-12)^-1/2) V^T
+  if (tid <= L) {
+    const int l = tid;
+    double S[kMaxN * kMaxN], V[kMaxN * kMaxN];  // one thread per l; local memory
+    // Gamma(l + 3/2) = (2l+1)!! sqrt(pi) / 2^(l+1)
+    double g = sqrt(kPi);
+    for (int k = 1; k <= 2 * l + 1; k += 2) g *= (double)k;
+    g /= pow(2.0, (double)(l + 1));
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) {
+        const double m = a.alpha[l * N + i] + a.alpha[l * N + j];
+        S[i * kMaxN + j] = 0.5 * g * pow(m, -((double)l + 1.5));
+        V[i * kMaxN + j] = (i == j) ? 1.0 : 0.0;
+      }
+    for (int sweep = 0; sweep < 60; ++sweep) {
+      double off = 0.0, diag = 0.0;
+      for (int i = 0; i < N; ++i) {
+        diag += S[i * kMaxN + i] * S[i * kMaxN + i];
+        for (int j = i + 1; j < N; ++j) off += S[i * kMaxN + j] * S[i * kMaxN + j];
+      }
+      if (off <= 1e-34 * diag) break;
+      for (int p = 0; p < N; ++p)
+        for (int q = p + 1; q < N; ++q) {
+          const double apq = S[p * kMaxN + q];
+          if (apq == 0.0) continue;
+          const double app = S[p * kMaxN + p], aqq = S[q * kMaxN + q];
+          const double theta = (aqq - app) / (2.0 * apq);
+          const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+          const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+          for (int k = 0; k < N; ++k) {  // columns p, q
+            const double akp = S[k * kMaxN + p], akq = S[k * kMaxN + q];
+            S[k * kMaxN + p] = c * akp - s * akq;
+            S[k * kMaxN + q] = s * akp + c * akq;
+          }
+          for (int k = 0; k < N; ++k) {  // rows p, q
+            const double apk = S[p * kMaxN + k], aqk = S[q * kMaxN + k];
+            S[p * kMaxN + k] = c * apk - s * aqk;
+            S[q * kMaxN + k] = s * apk + c * aqk;
+          }
+          for (int k = 0; k < N; ++k) {
+            const double vkp = V[k * kMaxN + p], vkq = V[k * kMaxN + q];
+            V[k * kMaxN + p] = c * vkp - s * vkq;
+            V[k * kMaxN + q] = s * vkp + c * vkq;
+          }
+        }
+    }
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) {
+        double acc = 0.0;
+        for (int k = 0; k < N; ++k) {
+          const double w = fmax(S[k * kMaxN + k], 1e-12);
+          acc += V[i * kMaxN + k] * V[j * kMaxN + k] / sqrt(w);
+        }
+        a.beta[(l * N + i) * N + j] = acc;
+      }
+  }
+  __syncthreads();
+
+  // Radial tables: Chebyshev interpolation at 8 nodes per segment, FP64.
+  for (int task = tid; task < a.nseg * NF; task += blockDim.x) {
+    const int seg = task / NF, fn = task % NF;
+    const int l = fn / N, n = fn % N;
+    double fb[kNCoef], fh[kNCoef];
+    for (int j = 0; j < kNCoef; ++j) {
+      const double tj = cos((2.0 * j + 1.0) * kPi / (2.0 * kNCoef));
+      const double r = (seg + 0.5 * (tj + 1.0)) * a.h;
+      double b = 0.0, bh = 0.0;
+      for (int k = 0; k < N; ++k) {
+        const double e = s_pref[l * kMaxN + k] * exp(-s_gamma[l * kMaxN + k] * r * r);
+        const double be = a.beta[(l * N + n) * N + k];
+        b += be * e;
+        bh += be * (-2.0 * s_gamma[l * kMaxN + k]) * e;
+      }
+      fb[j] = b;
+      fh[j] = bh;
+    }
+    for (int which = 0; which < 2; ++which) {
+      const double* f = which ? fh : fb;
+      double cheb[kNCoef];
+      for (int i = 0; i < kNCoef; ++i) {
+        double s = 0.0;
+        for (int j = 0; j < kNCoef; ++j) s += f[j] * cos(i * (2.0 * j + 1.0) * kPi / (2.0 * kNCoef));
+        cheb[i] = s * 2.0 / kNCoef;
+      }
+      cheb[0] *= 0.5;
+      // monomial coefficients: sum_i cheb_i T_i(t), T_{i+1} = 2 t T_i - T_{i-1}
+      double mono[kNCoef] = {0}, Tprev[kNCoef] = {0}, Tcur[kNCoef] = {0}, Tnext[kNCoef];
+      Tcur[0] = 1.0;  // T_0
+      for (int i = 0; i < kNCoef; ++i) {
+        for (int k = 0; k < kNCoef; ++k) mono[k] += cheb[i] * Tcur[k];
+        for (int k = 0; k < kNCoef; ++k)
+          Tnext[k] = (i == 0) ? (k == 1 ? 1.0 : 0.0) : (k > 0 ? 2.0 * Tcur[k - 1] : 0.0) - Tprev[k];
+        for (int k = 0; k < kNCoef; ++k) { Tprev[k] = Tcur[k]; Tcur[k] = Tnext[k]; }
+      }
+      float* dst = (which ? a.tab_bh : a.tab_b) + ((size_t)seg * NF + fn) * kNCoef;
+      for (int k = 0; k < kNCoef; ++k) dst[k] = (float)mono[k];
+    }
+  }
+  if (tid == 0) { a.err[0] = 0.0; a.err[1] = 0.0; }
+  __syncthreads();
+
+  // Table error: max |table - exact| / max |exact| per function, 17 points per segment.
+  for (int fn = tid; fn < NF; fn += blockDim.x) {
+    const int l = fn / N, n = fn % N;
+    double eb = 0.0, eh = 0.0, mb = 0.0, mh = 0.0;
+    for (int seg = 0; seg < a.nseg; ++seg) {
+      const float* cb = a.tab_b + ((size_t)seg * NF + fn) * kNCoef;
+      const float* ch = a.tab_bh + ((size_t)seg * NF + fn) * kNCoef;
+      for (int j = 0; j <= 16; ++j) {
+        const double t = -1.0 + j / 8.0;
+        const double r = (seg + 0.5 * (t + 1.0)) * a.h;
+        double b = 0.0, bh = 0.0;
+        for (int k = 0; k < N; ++k) {
+          const double e = s_pref[l * kMaxN + k] * exp(-s_gamma[l * kMaxN + k] * r * r);
+          const double be = a.beta[(l * N + n) * N + k];
+          b += be * e;
+          bh += be * (-2.0 * s_gamma[l * kMaxN + k]) * e;
+        }
+        double pb = cb[kDeg], ph = ch[kDeg];
+        for (int k = kDeg - 1; k >= 0; --k) { pb = pb * t + cb[k]; ph = ph * t + ch[k]; }
+        eb = fmax(eb, fabs(pb - b));
+        eh = fmax(eh, fabs(ph - bh));
+        mb = fmax(mb, fabs(b));
+        mh = fmax(mh, fabs(bh));
+      }
+    }
+    atomic_max_nonneg(&a.err[0], mb > 0 ? eb / mb : 0.0);
+    atomic_max_nonneg(&a.err[1], mh > 0 ? eh / mh : 0.0);
+  }
+
+  // Power-spectrum feature table in DScribe order (SG:1215-1245).
+  if (tid == 0) {
+    int off = 0, nb = 0;
+    const int S = a.S;
+    for (int j = 0; j < S; ++j)
+      for (int jd = j; jd < (a.crossover ? S : j + 1); ++jd)
+        for (int l = 0; l <= L; ++l) {
+          s_boff[nb++] = off;
+          off += (j == jd) ? N * (N + 1) / 2 : N * N;
+        }
+  }
+  __syncthreads();
+  {
+    const int S = a.S;
+    int b = 0;
+    for (int j = 0; j < S; ++j)
+      for (int jd = j; jd < (a.crossover ? S : j + 1); ++jd)
+        for (int l = 0; l <= L; ++l, ++b) {
+          if (b % blockDim.x != tid) continue;
+          int f = s_boff[b];
+          for (int n = 0; n < N; ++n)
+            for (int nd = (j == jd ? n : 0); nd < N; ++nd) a.ftab[f++] = fcode(j, jd, n, nd, l);
+        }
+  }
+}
+
+}  // namespace soapb
+
+using namespace soapb;
+
+extern "C" int soapb_basis_plan(soapb_basis* b) {
+  if (!b) return set_error(SOAPB_ERR_ARG, "null basis");
+  if (b->n_max < 1 || b->n_max > kMaxN) return set_error(SOAPB_ERR_ARG, "n_max must be in [1, %d]", kMaxN);
+  if (b->l_max < 0 || b->l_max > kMaxL) return set_error(SOAPB_ERR_ARG, "l_max must be in [0, %d]", kMaxL);
+  if (b->n_species < 1 || b->n_species > kMaxS)
+    return set_error(SOAPB_ERR_ARG, "n_species must be in [1, %d]", kMaxS);
+  if (!(b->r_cut > 0.0) || !(b->sigma > 0.0)) return set_error(SOAPB_ERR_ARG, "r_cut and sigma must be > 0");
+  const int N = b->n_max, L = b->l_max, S = b->n_species;
+  b->eta = 1.0 / (2.0 * b->sigma * b->sigma);
+  b->cutoff = b->r_cut + b->sigma * sqrt(-2.0 * log(1e-3));
+  double gmax = 0.0;
+  for (int l = 0; l <= L; ++l)
+    for (int n = 0; n < N; ++n) {
+      const double an = (N == 1) ? 1.0 : 1.0 + (b->r_cut - 1.0) * (double)n / (double)(N - 1);
+      const double al = -log(1e-3 / pow(an, (double)l)) / (an * an);
+      gmax = fmax(gmax, al * b->eta / (al + b->eta));
+    }
+  if (b->n_seg <= 0) {
+    int ns = (int)ceil(b->cutoff * sqrt(gmax) / 0.5);
+    b->n_seg = ns < 4 ? 4 : ns;
+  }
+  b->seg_width = b->cutoff / b->n_seg;
+  b->n_keys = S * b->n_seg;
+  if (b->n_keys > kMaxKeys) return set_error(SOAPB_ERR_ARG, "n_species * n_seg = %d exceeds %d", b->n_keys, kMaxKeys);
+  const int ch = S * N;
+  b->n_feat_ps = b->crossover ? ch * (ch + 1) / 2 * (L + 1) : S * (L + 1) * (N * (N + 1) / 2);
+  b->n_feat_cc = S * N * (L + 1) * (L + 1);
+  const int NF = N * (L + 1);
+  int64_t off = 0;
+  b->off_alpha = off; off = align_up(off + 8 * (int64_t)NF, 256);
+  b->off_beta = off; off = align_up(off + 8 * (int64_t)NF * N, 256);
+  b->off_tab_b = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
+  b->off_tab_bh = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
+  b->off_ftab = off; off = align_up(off + 4 * (int64_t)b->n_feat_ps, 256);
+  b->off_err = off; off = align_up(off + 16, 256);
+  b->bytes = off;
+  b->dev = nullptr;
+  return SOAPB_OK;
+}
+
+extern "C" int soapb_basis_build(soapb_basis* b, void* dev_buf, void* stream) {
+  if (!b || !dev_buf) return set_error(SOAPB_ERR_ARG, "null basis or buffer");
+  if (b->bytes <= 0) return set_error(SOAPB_ERR_ARG, "call soapb_basis_plan first");
+  if (((uintptr_t)dev_buf) % 256) return set_error(SOAPB_ERR_ARG, "basis buffer must be 256-byte aligned");
+  b->dev = dev_buf;
+  char* base = (char*)dev_buf;
+  BasisDev a;
+  a.N = b->n_max; a.L = b->l_max; a.S = b->n_species; a.crossover = b->crossover ? 1 : 0;
+  a.nseg = b->n_seg; a.F = b->n_feat_ps;
+  a.r_cut = b->r_cut; a.eta = b->eta; a.cutoff = b->cutoff; a.h = b->seg_width;
+  a.alpha = (double*)(base + b->off_alpha);
+  a.beta = (double*)(base + b->off_beta);
+  a.tab_b = (float*)(base + b->off_tab_b);
+  a.tab_bh = (float*)(base + b->off_tab_bh);
+  a.ftab = (int*)(base + b->off_ftab);
+  a.err = (double*)(base + b->off_err);
+  k_basis_build<<<1, 256, 0, (cudaStream_t)stream>>>(a);
+  return check_launch("k_basis_build");
+}
+
+extern "C" int soapb_basis_download(const soapb_basis* b, double* h_alpha, double* h_beta, double* h_err2,
+                                    void* stream) {
+  if (!b || !b->dev) return set_error(SOAPB_ERR_ARG, "basis not built");
+  const int NF = b->n_max * (b->l_max + 1);
+  cudaStream_t st = (cudaStream_t)stream;
+  const char* base = (const char*)b->dev;
+  int rc;
+  if (h_alpha && (rc = check_cuda(cudaMemcpyAsync(h_alpha, base + b->off_alpha, 8 * (size_t)NF,
+                                                  cudaMemcpyDeviceToHost, st), "alpha download")))
+    return rc;
+  if (h_beta && (rc = check_cuda(cudaMemcpyAsync(h_beta, base + b->off_beta, 8 * (size_t)NF * b->n_max,
+                                                 cudaMemcpyDeviceToHost, st), "beta download")))
+    return rc;
+  if (h_err2 && (rc = check_cuda(cudaMemcpyAsync(h_err2, base + b->off_err, 16, cudaMemcpyDeviceToHost, st),
+                                 "err download")))
+    return rc;
+  return check_cuda(cudaStreamSynchronize(st), "basis download sync");
+}

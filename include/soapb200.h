@@ -1,0 +1,180 @@
+/*
+ * soapb200.h -- C ABI of the B200 SOAP descriptor library (libsoapb200.so).
+ *
+ * The library replaces the compute path of the reference SOAP generator
+ * (TACC/cuSOAP, src/cusoap/soap_generator.py, cited as SG:<line>): the
+ * radius neighbour search, the GTO coefficient accumulation, the power
+ * spectrum / cc projection, the closed-form Jacobian and the force adjoint.
+ * The reference exposes these only as private methods of its Python SOAP
+ * class; the Python package cusoap_b200 binds the functions below with
+ * ctypes and keeps the reference's public SOAP(...) / create() /
+ * derivatives() surface.
+ *
+ * Conventions
+ *  - Every pointer named dev_* / d_* is device memory owned by the caller.
+ *    The library performs no device allocation of its own; work buffers are
+ *    passed in, with their sizes queried beforehand.
+ *  - All work is enqueued on the given CUDA stream (cudaStream_t passed as
+ *    void*; NULL = legacy default stream); functions return once enqueued.
+ *  - Functions return SOAPB_OK (0) or an error status; soapb_last_error()
+ *    gives a message for the calling thread.  No C++ exception crosses the
+ *    ABI.  A handle (soapb_basis) is not thread-safe; use one per thread or
+ *    stream, as the reference's SOAP object is (SG:1921-1922).
+ *  - Positions, cells and centre coordinates are float64 (the reference
+ *    computes internally in float64, SG:1775-1780); the bulk arithmetic and
+ *    all outputs are float32.
+ */
+#ifndef SOAPB200_H
+#define SOAPB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SOAPB_OK = 0,
+  SOAPB_ERR_ARG = 1,         /* invalid argument or unsupported size */
+  SOAPB_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  SOAPB_ERR_CAPACITY = 3,    /* an output buffer was too small; retry bigger */
+  SOAPB_ERR_UNSUPPORTED = 4, /* parameter combination not built */
+  SOAPB_ERR_ACCURACY = 5     /* radial tables missed their error bound */
+};
+
+/* average / output modes of the descriptor */
+enum {
+  SOAPB_OUT_PS = 0,  /* power spectrum, DScribe order (average off/inner/outer, SG:1634-1689) */
+  SOAPB_OUT_CC = 1,  /* projection coefficients, DScribe cc layout (SG:1603-1632) */
+  SOAPB_OUT_RAW = 2  /* c[s][n][lm] per centre, no permutation / scaling */
+};
+
+/* GTO basis + radial tables.  Fill the five input fields, call
+ * soapb_basis_plan (host only) to get the sizes, allocate `bytes` of device
+ * memory, then soapb_basis_build.  Replaces SOAP.__init__'s basis set-up:
+ * _init_gto_basis SG:690-708, _lowdin_invsqrt SG:339-343, the cutoff
+ * padding SG:600-602 and the feature tables SG:1215-1291. */
+typedef struct soapb_basis {
+  /* inputs */
+  int32_t n_max, l_max, n_species, crossover;
+  double r_cut, sigma;
+  /* derived by soapb_basis_plan */
+  double eta;        /* 1 / (2 sigma^2) */
+  double cutoff;     /* r_cut + sigma sqrt(-2 ln 1e-3) */
+  double seg_width;  /* radial table segment width (A) */
+  int32_t n_seg;     /* radial table segments over [0, cutoff] */
+  int32_t n_keys;    /* n_species * n_seg: neighbour sort keys */
+  int32_t n_feat_ps; /* SG:913-919 */
+  int32_t n_feat_cc; /* SG:909-910 */
+  int64_t bytes;     /* device bytes the basis needs */
+  int64_t off_alpha, off_beta, off_tab_b, off_tab_bh, off_ftab, off_err;
+  void* dev;         /* set by soapb_basis_build */
+} soapb_basis;
+
+int soapb_basis_plan(soapb_basis* b);
+int soapb_basis_build(soapb_basis* b, void* dev_buf, void* stream);
+/* Copy the FP64 alpha (l_max+1, n_max), beta (l_max+1, n_max, n_max) and the
+ * two table errors (max |table - exact| / max|exact| for B and Bhat) to host
+ * memory; synchronises the stream. */
+int soapb_basis_download(const soapb_basis* b, double* h_alpha, double* h_beta, double* h_err2, void* stream);
+
+/* A batch of structures.  Atoms of structure i are [atom_off[i], atom_off[i+1]).
+ * cells: (n_struct, 3, 3) row vectors (lattice a, b, c); pbc: (n_struct, 3).
+ * Structures whose pbc is all zero ignore their cell. */
+typedef struct soapb_structs {
+  int32_t n_struct;
+  int64_t n_atoms;
+  const int64_t* d_atom_off;   /* (n_struct + 1) */
+  const double* d_positions;   /* (n_atoms, 3) */
+  const int32_t* d_species;    /* (n_atoms,) species index in [0, n_species) */
+  const double* d_cells;       /* (n_struct, 9) */
+  const uint8_t* d_pbc;        /* (n_struct, 3) */
+} soapb_structs;
+
+/* Centres: one row per output descriptor row.
+ * centre_atom >= 0 marks an index centre (or a Cartesian centre that
+ * coincides with that atom, SG:966-1003); its own r=0 edge then carries the
+ * analytic self term (SG:765-850). */
+typedef struct soapb_centres {
+  int64_t n_centres;
+  const double* d_xyz;         /* (n_centres, 3) */
+  const int32_t* d_struct;     /* (n_centres,) structure of each centre */
+  const int32_t* d_atom;       /* (n_centres,) centre atom or -1 */
+} soapb_centres;
+
+/* Neighbour pairs, CSR over centres, pairs of a centre sorted by
+ * (neighbour species, radial segment).  One pair = float4
+ * {rx, ry, rz, bits(atom | species << 27)}, r = neighbour - centre. */
+enum {
+  SOAPB_NL_CREATE = 0,   /* drop r <= 1e-12 edges except the centre's own (SG:1171-1179) */
+  SOAPB_NL_ALL = 1       /* keep every edge within the cutoff (SG:2372-2373) */
+};
+
+/* Workspace bytes for soapb_neighbors_count / _fill (cell lists, scan). */
+int soapb_neighbors_workspace(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c,
+                              int64_t* bytes);
+/* Bins the atoms into cell lists (counting sort), counts the pairs of every
+ * centre and writes the exclusive scan d_pair_off (n_centres + 1).  The
+ * total pair count is d_pair_off[n_centres].  Replaces _radius_edges /
+ * _build_neighbor_list / _extend_periodic (SG:1015-1181). */
+int soapb_neighbors_count(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c, int32_t mode,
+                          void* d_work, int64_t work_bytes, int64_t* d_pair_off, void* stream);
+/* Writes the sorted pairs (capacity = allocated pairs).  Must follow
+ * soapb_neighbors_count with the same arguments and workspace. */
+int soapb_neighbors_fill(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c, int32_t mode,
+                         void* d_work, int64_t work_bytes, const int64_t* d_pair_off, void* d_pairs,
+                         int64_t capacity, void* stream);
+/* Error flags of the last count/fill on this workspace (synchronises the
+ * stream): bit 0 singular cell, bit 1 atom more than 511 cells outside its
+ * cell, bit 2 pair capacity exceeded.  0 = no error. */
+int soapb_neighbors_status(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c, void* d_work,
+                           int32_t* h_status, void* stream);
+
+/* Descriptor: fused radial x solid-harmonic accumulation of c_nlm per centre
+ * in registers, then the power spectrum / cc / raw epilogue, one warp per
+ * centre from a work queue.  d_out: (n_centres, F) float32 with
+ * F = n_feat_ps (PS), n_feat_cc (CC, RAW).  d_coeff: optional (may be NULL)
+ * second output of the raw c[s][n][lm] rows (n_centres, n_feat_cc), as the
+ * derivative and adjoint paths need.  d_counter: one int32 of scratch.
+ * Replaces _coefficients_gto SG:1294-1391, _add_self_terms SG:821-850,
+ * _power_spectrum SG:1634-1689 and _projection_cc SG:1624-1632. */
+int soapb_descriptor(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
+                     int32_t out_mode, float* d_out, float* d_coeff, int32_t* d_counter, void* stream);
+
+/* Dense Jacobian of the descriptor w.r.t. the included atoms: d_out
+ * (n_centres, n_inc, 3, F) float32, every element written once (zeros
+ * included).  d_coeff: raw coefficients (soapb_descriptor's d_coeff) on the
+ * same SOAPB_NL_ALL pairs.  d_inc_row: (n_atoms,) output row of each atom or
+ * -1.  attach = 0: fixed centres (DScribe convention, SG:2297-2301); 1:
+ * centres move with their atom (d_centre_atom), adding the centre-motion
+ * term.  max_pairs: upper bound on the pairs of any centre.  out_mode PS or
+ * CC.  d_status: int32 flag, nonzero if a centre exceeded the kernel's
+ * staging capacity.  Every edge of an atom accumulates, so periodic images
+ * are handled.  Replaces derivatives_analytical_ps SG:2270-2626 and its
+ * Triton kernels SG:50-220. */
+int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
+                   const float* d_coeff, const int32_t* d_inc_row, int64_t n_inc, const int32_t* d_centre_atom,
+                   int32_t attach, int32_t max_pairs, int32_t out_mode, float* d_out, int32_t* d_status,
+                   void* stream);
+
+/* Adjoint: given dE/dp (n_centres, n_feat_ps) float32, accumulate
+ * d_forces[a] += -dE/dx_a (float32 (n_atoms, 3); the caller zeroes it) with
+ * float atomics.  attach = 1: centres move with their atoms (d_centre_atom);
+ * 0: fixed centres.  d_coeff: raw coefficients on SOAPB_NL_ALL pairs.
+ * d_counter: one int32 of scratch.  Replaces one reverse pass of the
+ * reference's autograd Jacobian SG:2007-2113 without materialising dp/dr. */
+int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
+                 const float* d_coeff, const float* d_dEdp, const int32_t* d_centre_atom, int32_t attach,
+                 float* d_forces, int32_t* d_counter, void* stream);
+
+/* Message describing the last error on the calling thread ("" if none). */
+const char* soapb_last_error(void);
+/* Library version string. */
+const char* soapb_version(void);
+/* Number of kernels this library has launched in the process so far. */
+int64_t soapb_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SOAPB200_H */

@@ -1,0 +1,70 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports
+every symbol the header declares, and the host-only planning function agrees
+with the oracle's feature bookkeeping."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from cusoap_b200 import _lib, workloads as W
+from oracle.soap_oracle import OracleSOAP
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _header_symbols():
+    txt = open(os.path.join(ROOT, "include", "soapb200.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(soapb_\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_library_exports_every_header_symbol():
+    lib = _lib.load()
+    syms = _header_symbols()
+    assert len(syms) >= 12
+    for name in syms:
+        assert hasattr(lib, name), name
+    assert set(syms) == set(_lib.EXPORTS)
+    assert "sm_100a" in _lib.version()
+
+
+@pytest.mark.parametrize("name", list(W.CONFIGS))
+def test_basis_plan_matches_oracle(name):
+    P = W.CONFIGS[name]
+    lib = _lib.load()
+    b = _lib.Basis()
+    b.n_max, b.l_max, b.n_species, b.crossover = P["n_max"], P["l_max"], len(P["species"]), 1
+    b.r_cut, b.sigma = P["r_cut"], P["sigma"]
+    _lib.check(lib.soapb_basis_plan(ctypes.byref(b)))
+    o = OracleSOAP(**{k: v for k, v in P.items() if k != "periodic"})
+    assert b.n_feat_ps == o.n_power_features()
+    assert b.n_feat_cc == len(P["species"]) * P["n_max"] * (P["l_max"] + 1) ** 2
+    assert abs(b.cutoff - o.cutoff) < 1e-12
+    assert abs(b.eta - o.eta) < 1e-15
+    assert b.n_seg * b.seg_width == pytest.approx(b.cutoff)
+    assert b.bytes > 0 and b.off_err + 16 <= b.bytes
+
+
+def test_basis_plan_rejects_bad_sizes():
+    lib = _lib.load()
+    b = _lib.Basis()
+    b.n_max, b.l_max, b.n_species, b.crossover, b.r_cut, b.sigma = 4, 12, 1, 1, 5.0, 0.5
+    st = lib.soapb_basis_plan(ctypes.byref(b))
+    assert st == _lib.ERR_ARG
+    assert "l_max" in lib.soapb_last_error().decode()
+    b.l_max, b.n_max = 3, 0
+    assert lib.soapb_basis_plan(ctypes.byref(b)) == _lib.ERR_ARG
+
+
+def test_device_entry_points_validate_before_launch():
+    """Null-argument checks run on the host and never touch the device."""
+    lib = _lib.load()
+    b = _lib.Basis()
+    assert lib.soapb_descriptor(ctypes.byref(b), 10, None, None, 0, None, None, None, None) == _lib.ERR_ARG
+    assert lib.soapb_forces(ctypes.byref(b), 10, None, None, None, None, None, 1, None, None, None) == _lib.ERR_ARG
+
+
+def test_soap_requires_cuda_device():
+    from cusoap_b200 import SOAP
+    with pytest.raises(ValueError):
+        SOAP(species=[1], r_cut=3.0, n_max=2, l_max=1, device="cpu")
