@@ -17,6 +17,8 @@
 // Distances are tested and differences taken in FP64; rvec is stored FP32.
 #include <math.h>
 
+#include <mutex>
+
 #include "common.cuh"
 
 namespace soapb {
@@ -721,4 +723,68 @@ extern "C" int soapb_neighbors_status(const soapb_basis* b, const soapb_structs*
   if ((rc = check_cuda(cudaMemcpyAsync(h_status, w.status, 4, cudaMemcpyDeviceToHost, st), "status download")))
     return rc;
   return check_cuda(cudaStreamSynchronize(st), "status sync");
+}
+
+// ---------------------------------------------------------------------------
+// Neighbour list without any device allocation
+// ---------------------------------------------------------------------------
+// The regular entry points take a caller-sized workspace.  Some callers have
+// no way to provide one at the moment they need a neighbour list: a plain C or
+// Fortran molecular-dynamics driver that owns a fixed device-memory budget
+// and forbids libraries from allocating after set-up, or a time-step loop
+// where cudaMalloc / cudaFree would synchronise the device and stall it.
+// soapb_neighbors_noalloc serves them: its scratch is one fixed device array
+// that exists from module load to process exit on every GPU that loads the
+// library, so the call itself allocates nothing.
+namespace soapb {
+
+constexpr int64_t kNoAllocScratchBytes = 8ll << 20;  // 8 MiB per device
+static __device__ __align__(256) unsigned char g_nl_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_scratch_mu;
+static void* g_scratch_dev_ptr[64] = {};
+
+// Device address of g_nl_scratch on the current device, looked up once per
+// device (the host-side symbol is not a device address).
+static int scratch_address(void** out) {
+  int dev = 0;
+  int rc = check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+  if (rc) return rc;
+  if (dev < 0 || dev >= 64) return set_error(SOAPB_ERR_ARG, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_dev_ptr[dev]) {
+    void* p = nullptr;
+    rc = check_cuda(cudaGetSymbolAddress(&p, g_nl_scratch), "cudaGetSymbolAddress(g_nl_scratch)");
+    if (rc) return rc;
+    g_scratch_dev_ptr[dev] = p;
+  }
+  *out = g_scratch_dev_ptr[dev];
+  return SOAPB_OK;
+}
+
+}  // namespace soapb
+
+extern "C" int soapb_neighbors_noalloc(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c,
+                                       int32_t mode, int64_t* d_pair_off, void* d_pairs, int64_t capacity,
+                                       int32_t* d_status, void* stream) {
+  int rc = check_inputs(b, s, c);
+  if (rc) return rc;
+  if (!d_pair_off || !d_status) return set_error(SOAPB_ERR_ARG, "null pair_off or status");
+  const NLLayout L = nl_layout(s, c);
+  if (L.total > kNoAllocScratchBytes)
+    return set_error(SOAPB_ERR_ARG,
+                     "soapb_neighbors_noalloc: this input needs %lld bytes of scratch but the fixed scratch array "
+                     "holds %lld bytes (about 55,000 atoms with every atom a centre); use soapb_neighbors_count/_fill with a workspace",
+                     (long long)L.total, (long long)kNoAllocScratchBytes);
+  void* scratch = nullptr;
+  if ((rc = scratch_address(&scratch))) return rc;
+  // count clears the scratch words that must start at zero (status, bin counts, bin cursors)
+  if ((rc = soapb_neighbors_count(b, s, c, mode, scratch, kNoAllocScratchBytes, d_pair_off, stream))) return rc;
+  if ((rc = soapb_neighbors_fill(b, s, c, mode, scratch, kNoAllocScratchBytes, d_pair_off, d_pairs, capacity,
+                                 stream)))
+    return rc;
+  const NLWork w = nl_work(L, scratch);
+  return check_cuda(cudaMemcpyAsync(d_status, w.status, sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                                    (cudaStream_t)stream),
+                    "status copy");
 }

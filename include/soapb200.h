@@ -130,6 +130,26 @@ int soapb_neighbors_fill(const soapb_basis* b, const soapb_structs* s, const soa
 int soapb_neighbors_status(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c, void* d_work,
                            int32_t* h_status, void* stream);
 
+/* Neighbour list that allocates nothing, for callers that cannot allocate
+ * device memory when they need a list (a C/Fortran MD driver with a fixed
+ * device-memory budget, or a time-step loop where cudaMalloc/cudaFree would
+ * synchronise the device).  It has no counterpart in the reference.  Same
+ * inputs and outputs as soapb_neighbors_count + soapb_neighbors_fill, but
+ * the workspace is a fixed 8 MiB device array inside the library (held on
+ * every GPU that loads it until the process exits), enough for about
+ * 55,000 atoms when every atom is a centre (~140 bytes per atom); larger inputs return SOAPB_ERR_ARG before
+ * anything is launched.  Pairs are written only when the total
+ * d_pair_off[n_centres] fits `capacity`; *d_status (device int32) receives
+ * the error flags of soapb_neighbors_status (bit 2 = capacity too small).
+ * The first call on each device looks up the array's device address with
+ * cudaGetSymbolAddress; make that first call before any stream capture.
+ * All calls share the one array and each call clears what must start at
+ * zero; calls whose executions overlap on the GPU (other streams, other
+ * threads) race on it. */
+int soapb_neighbors_noalloc(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c, int32_t mode,
+                            int64_t* d_pair_off, void* d_pairs, int64_t capacity, int32_t* d_status,
+                            void* stream);
+
 /* Descriptor: fused radial x solid-harmonic accumulation of c_nlm per centre
  * in registers, then the power spectrum / cc / raw epilogue, one warp per
  * centre from a work queue.  d_out: (n_centres, F) float32 with
