@@ -20,7 +20,7 @@ EXPORTS = (
     "soapb_basis_plan", "soapb_basis_build", "soapb_basis_download",
     "soapb_neighbors_workspace", "soapb_neighbors_count", "soapb_neighbors_fill", "soapb_neighbors_status",
     "soapb_neighbors_noalloc",
-    "soapb_descriptor", "soapb_jacobian", "soapb_forces",
+    "soapb_descriptor", "soapb_jacobian_workspace", "soapb_jacobian", "soapb_forces",
     "soapb_last_error", "soapb_version", "soapb_kernel_launches",
 )
 
@@ -81,7 +81,9 @@ def load() -> ctypes.CDLL:
         "soapb_neighbors_noalloc": [POINTER(Basis), POINTER(Structs), POINTER(Centres), c_int32, P, P, c_int64, P,
                                     P],
         "soapb_descriptor": [POINTER(Basis), c_int64, P, P, c_int32, P, P, P, P],
-        "soapb_jacobian": [POINTER(Basis), c_int64, P, P, P, P, c_int64, P, c_int32, c_int32, c_int32, P, P, P],
+        "soapb_jacobian_workspace": [POINTER(Basis), c_int64, c_int64, c_int64, c_int32, POINTER(c_int64)],
+        "soapb_jacobian": [POINTER(Basis), c_int64, P, P, c_int64, P, P, c_int64, P, c_int32, c_int32, c_int32, P,
+                           P, c_int64, P, P],
         "soapb_forces": [POINTER(Basis), c_int64, P, P, P, P, P, c_int32, P, P, P],
     }
     for name, args in sig.items():

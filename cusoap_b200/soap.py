@@ -486,10 +486,14 @@ class SOAP:
                 inc_row = inc_row.to(self.device)
                 status = torch.zeros(1, dtype=torch.int32, device=self.device)
                 lib = _lib.load()
+                wsb = ctypes.c_int64(0)
+                check(lib.soapb_jacobian_workspace(ctypes.byref(self._basis), batch.n_centres, pairs.total, n_inc,
+                                                   int(bool(attach)), ctypes.byref(wsb)))
+                work = torch.empty(max(int(wsb.value), 256), dtype=torch.uint8, device=self.device)
                 self._call("jacobian", lib.soapb_jacobian, ctypes.byref(self._basis), batch.n_centres,
-                           _ptr(pairs.pair_off), _ptr(pairs.pairs), _ptr(coeff), _ptr(inc_row), n_inc,
+                           _ptr(pairs.pair_off), _ptr(pairs.pairs), pairs.total, _ptr(coeff), _ptr(inc_row), n_inc,
                            _ptr(batch.centre_attach), int(bool(attach)), pairs.max_pairs, mode,
-                           _ptr(deriv), _ptr(status), _stream(self.device))
+                           _ptr(deriv), _ptr(work), work.numel(), _ptr(status), _stream(self.device))
                 if int(status.item()) != 0:
                     raise _lib.SoapbError(_lib.ERR_CAPACITY, "jacobian staging capacity exceeded")
             if self.dtype != torch.float32:

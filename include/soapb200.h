@@ -67,7 +67,7 @@ typedef struct soapb_basis {
   int32_t n_feat_ps; /* SG:913-919 */
   int32_t n_feat_cc; /* SG:909-910 */
   int64_t bytes;     /* device bytes the basis needs */
-  int64_t off_alpha, off_beta, off_tab_b, off_tab_bh, off_ftab, off_err;
+  int64_t off_alpha, off_beta, off_tab_b, off_tab_bh, off_ftab, off_err;  /* byte offsets into dev */
   void* dev;         /* set by soapb_basis_build */
 } soapb_basis;
 
@@ -161,21 +161,25 @@ int soapb_neighbors_noalloc(const soapb_basis* b, const soapb_structs* s, const 
 int soapb_descriptor(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
                      int32_t out_mode, float* d_out, float* d_coeff, int32_t* d_counter, void* stream);
 
+/* Workspace bytes of soapb_jacobian (sorted per-centre entries, a nonzero-row
+ * bitmap, a work counter) for n_pairs = d_pair_off[n_centres] pairs. */
+int soapb_jacobian_workspace(const soapb_basis* b, int64_t n_centres, int64_t n_pairs, int64_t n_inc,
+                             int32_t attach, int64_t* bytes);
 /* Dense Jacobian of the descriptor w.r.t. the included atoms: d_out
- * (n_centres, n_inc, 3, F) float32, every element written once (zeros
- * included).  d_coeff: raw coefficients (soapb_descriptor's d_coeff) on the
- * same SOAPB_NL_ALL pairs.  d_inc_row: (n_atoms,) output row of each atom or
- * -1.  attach = 0: fixed centres (DScribe convention, SG:2297-2301); 1:
- * centres move with their atom (d_centre_atom), adding the centre-motion
- * term.  max_pairs: upper bound on the pairs of any centre.  out_mode PS or
- * CC.  d_status: int32 flag, nonzero if a centre exceeded the kernel's
- * staging capacity.  Every edge of an atom accumulates, so periodic images
- * are handled.  Replaces derivatives_analytical_ps SG:2270-2626 and its
- * Triton kernels SG:50-220. */
+ * (n_centres, n_inc, 3, F) float32 (16-byte aligned), every element written
+ * once (zeros included).  d_coeff: raw coefficients (soapb_descriptor's
+ * d_coeff) on the same SOAPB_NL_ALL pairs.  d_inc_row: (n_atoms,) output row
+ * of each atom or -1.  attach = 0: fixed centres (DScribe convention,
+ * SG:2297-2301); 1: centres move with their atom (d_centre_atom), adding the
+ * centre-motion term.  max_pairs: upper bound on the pairs of any centre.
+ * out_mode PS or CC.  d_status: int32 flag, nonzero if a centre exceeded the
+ * kernel's staging capacity.  Every edge of an atom accumulates, so periodic
+ * images are handled.  Replaces derivatives_analytical_ps SG:2270-2626 and
+ * its Triton kernels SG:50-220. */
 int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
-                   const float* d_coeff, const int32_t* d_inc_row, int64_t n_inc, const int32_t* d_centre_atom,
-                   int32_t attach, int32_t max_pairs, int32_t out_mode, float* d_out, int32_t* d_status,
-                   void* stream);
+                   int64_t n_pairs, const float* d_coeff, const int32_t* d_inc_row, int64_t n_inc,
+                   const int32_t* d_centre_atom, int32_t attach, int32_t max_pairs, int32_t out_mode, float* d_out,
+                   void* d_work, int64_t work_bytes, int32_t* d_status, void* stream);
 
 /* Adjoint: given dE/dp (n_centres, n_feat_ps) float32, accumulate
  * d_forces[a] += -dE/dx_a (float32 (n_atoms, 3); the caller zeroes it) with

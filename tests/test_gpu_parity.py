@@ -90,6 +90,27 @@ def test_derivatives_full_cluster192_vs_oracle():
     assert _row_err(_np(J[cen]), Jo) < DERIV_TOL
     Do = o.create(s["positions"], s["atomic_numbers"])
     assert _row_err(_np(D), Do) < DESC_TOL
+    # attach=True (centre-motion term) on the same variant
+    Ja = gs.derivatives(s, centers=[3, 77], attach=True, return_descriptor=False)
+    Jf = gs.derivatives(s, centers=[3, 77], attach=False, return_descriptor=False)
+    Ja, Jf = _np(Ja).astype(np.float64), _np(Jf).astype(np.float64)
+    diff = Ja - Jf
+    # attach changes only the centre atom's row: -(sum of every fixed-centre row) ...
+    scale = np.abs(Jf[0]).max()
+    assert np.abs(np.delete(diff[0], 3, axis=0)).max() <= 1e-6 * scale
+    assert np.abs(diff[0, 3] + Jf[0].sum(0)).max() <= 1e-4 * scale
+    # ... so with attached centres the rows sum to zero (translation invariance)
+    assert np.abs(Ja[1].sum(0)).max() <= 1e-4 * np.abs(Ja[1]).max()
+
+
+def test_periodic_attach_translation_invariance():
+    """Periodic cell, attached centres, every atom included: the Jacobian rows
+    of a centre sum to zero (moving every atom moves every centre)."""
+    cell = W.random_cells(1, seed=17, a_min=30, a_max=30)[0]
+    s = _soap("waterbox2001", species=[1, 6, 7, 8])
+    J = _np(s.derivatives(cell, centers=[0, 5, 9], attach=True, return_descriptor=False)).astype(np.float64)
+    for k in range(3):
+        assert np.abs(J[k].sum(0)).max() <= 1e-4 * np.abs(J[k]).max()
 
 
 def test_periodic_cells_golden(golden):
