@@ -312,7 +312,7 @@ def run_ours(args):
     peak, peak_kind = _peaks()
     achieved = jac_bytes / (jac_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": _traffic_from_profiles(), "kernel": "k_jacobian<3>",
+                "traffic": _traffic_from_profiles() if args.nx == 10 else None, "kernel": "k_jacobian<3>",
                 "peak_kind": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s",
                 "algorithmic_bytes_per_launch": jac_bytes, "ms_per_launch": jac_ms,

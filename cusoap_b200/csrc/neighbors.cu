@@ -550,6 +550,30 @@ __global__ void __launch_bounds__(128) k_fill(VisitArgs A, int64_t n_centres, co
   }
 }
 
+// One block: total pairs, the largest per-centre count and the status flags,
+// so the host learns all three from one device-to-host copy.
+__global__ void __launch_bounds__(1024) k_stats(const int64_t* pair_off, int64_t n_centres, const int* status,
+                                                int64_t* out) {
+  __shared__ int64_t s_max[32];
+  int64_t m = 0;
+  for (int64_t c = threadIdx.x; c < n_centres; c += blockDim.x) {
+    const int64_t d = pair_off[c + 1] - pair_off[c];
+    m = d > m ? d : m;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const int64_t v = __shfl_xor_sync(0xffffffffu, m, o);
+    m = v > m ? v : m;
+  }
+  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) m = s_max[i] > m ? s_max[i] : m;
+    out[0] = pair_off[n_centres];
+    out[1] = m;
+    out[2] = status[0];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -723,6 +747,17 @@ extern "C" int soapb_neighbors_status(const soapb_basis* b, const soapb_structs*
   if ((rc = check_cuda(cudaMemcpyAsync(h_status, w.status, 4, cudaMemcpyDeviceToHost, st), "status download")))
     return rc;
   return check_cuda(cudaStreamSynchronize(st), "status sync");
+}
+
+extern "C" int soapb_neighbors_stats(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c,
+                                     const void* d_work, const int64_t* d_pair_off, int64_t* d_stats, void* stream) {
+  int rc = check_inputs(b, s, c);
+  if (rc) return rc;
+  if (!d_work || !d_pair_off || !d_stats) return set_error(SOAPB_ERR_ARG, "null workspace, pair_off or stats");
+  const NLLayout L = nl_layout(s, c);
+  const NLWork w = nl_work(L, const_cast<void*>(d_work));
+  k_stats<<<1, 1024, 0, (cudaStream_t)stream>>>(d_pair_off, c->n_centres, w.status, d_stats);
+  return check_launch("k_stats");
 }
 
 // ---------------------------------------------------------------------------

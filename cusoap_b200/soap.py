@@ -135,20 +135,21 @@ class _Pairs:
         self.pair_off = torch.empty(batch.n_centres + 1, dtype=torch.int64, device=dev)
         soap._call("neighbors_count", lib.soapb_neighbors_count, b, ctypes.byref(batch.cs), ctypes.byref(batch.cc),
                    mode, _ptr(self.work), self.work.numel(), _ptr(self.pair_off), st)
-        self.total = int(self.pair_off[-1].item())
+        # one device->host read: total pairs, largest per-centre count, status flags
+        stats = torch.empty(3, dtype=torch.int64, device=dev)
+        soap._call("neighbors_stats", lib.soapb_neighbors_stats, b, ctypes.byref(batch.cs), ctypes.byref(batch.cc),
+                   _ptr(self.work), _ptr(self.pair_off), _ptr(stats), st)
+        self.total, self.max_pairs, status = (int(v) for v in stats.cpu().tolist())
+        if status & 1:
+            raise ValueError("singular cell in a periodic structure")
+        if status & 2:
+            raise ValueError("an atom lies more than 511 cells outside its periodic cell")
+        if status:
+            raise _lib.SoapbError(_lib.ERR_CAPACITY, f"neighbour list status {status}")
+        # the list is allocated to the exact total, so the fill cannot overflow it
         self.pairs = torch.empty((max(self.total, 1), 4), dtype=torch.float32, device=dev)
         soap._call("neighbors_fill", lib.soapb_neighbors_fill, b, ctypes.byref(batch.cs), ctypes.byref(batch.cc),
                    mode, _ptr(self.work), self.work.numel(), _ptr(self.pair_off), _ptr(self.pairs), self.total, st)
-        status = ctypes.c_int32(0)
-        check(lib.soapb_neighbors_status(b, ctypes.byref(batch.cs), ctypes.byref(batch.cc), _ptr(self.work),
-                                         ctypes.byref(status), st))
-        if status.value & 1:
-            raise ValueError("singular cell in a periodic structure")
-        if status.value & 2:
-            raise ValueError("an atom lies more than 511 cells outside its periodic cell")
-        if status.value:
-            raise _lib.SoapbError(_lib.ERR_CAPACITY, f"neighbour list status {status.value}")
-        self.max_pairs = int((self.pair_off[1:] - self.pair_off[:-1]).max().item()) if batch.n_centres else 0
 
 
 class _SOAPFunction(torch.autograd.Function):

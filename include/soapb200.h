@@ -130,6 +130,15 @@ int soapb_neighbors_fill(const soapb_basis* b, const soapb_structs* s, const soa
 int soapb_neighbors_status(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c, void* d_work,
                            int32_t* h_status, void* stream);
 
+/* Summary of a neighbour list after soapb_neighbors_count (and, optionally,
+ * _fill), for one device-to-host read: d_stats (device int64[3]) receives
+ * {total pairs = d_pair_off[n_centres], largest pair count of a centre,
+ * status flags as soapb_neighbors_status}.  Stream-ordered, no sync.  No
+ * single counterpart in the reference: it replaces the edge-count and
+ * max-degree reads around _build_neighbor_list (soap_generator.py:1128-1181). */
+int soapb_neighbors_stats(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c, const void* d_work,
+                          const int64_t* d_pair_off, int64_t* d_stats, void* stream);
+
 /* Neighbour list that allocates nothing, for callers that cannot allocate
  * device memory when they need a list (a C/Fortran MD driver with a fixed
  * device-memory budget, or a time-step loop where cudaMalloc/cudaFree would
