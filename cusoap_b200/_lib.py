@@ -33,7 +33,7 @@ class Basis(ctypes.Structure):
         ("n_seg", c_int32), ("n_keys", c_int32), ("n_feat_ps", c_int32), ("n_feat_cc", c_int32),
         ("bytes", c_int64),
         ("off_alpha", c_int64), ("off_beta", c_int64), ("off_tab_b", c_int64), ("off_tab_bh", c_int64),
-        ("off_ftab", c_int64), ("off_err", c_int64),
+        ("off_ftab", c_int64), ("off_widx", c_int64), ("off_err", c_int64),
         ("dev", c_void_p),
     ]
 

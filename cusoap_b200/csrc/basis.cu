@@ -30,6 +30,7 @@ struct BasisDev {
   float* tab_b;
   float* tab_bh;
   int* ftab;
+  int* widx;
   double* err;
 };
 
@@ -186,6 +187,12 @@ __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
     atomic_max_nonneg(&a.err[1], mh > 0 ? eh / mh : 0.0);
   }
 
+  // Adjoint index table: widx[(l SN + b) SN + a] = feature of the pair {a, b} at l,
+  // a = j N + n, bit 30 set on a == b (d(c_a c_a) = 2 c_a), -1 where no feature exists.
+  {
+    const int SN = a.S * N;
+    for (int i = tid; i < (L + 1) * SN * SN; i += blockDim.x) a.widx[i] = -1;
+  }
   // Power-spectrum feature table in DScribe order (SG:1215-1245).
   if (tid == 0) {
     int off = 0, nb = 0;
@@ -210,6 +217,9 @@ __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
             for (int nd = (j == jd ? n : 0); nd < N; ++nd) {
               // second table: l-major coefficient-pair indices (l S + j) N + n, (l S + j') N + n', and l
               a.ftab[a.F + f] = ((l * S + j) * N + n) | (((l * S + jd) * N + nd) << 12) | (l << 24);
+              const int SN = S * N, ia = j * N + n, ib = jd * N + nd;
+              a.widx[(l * SN + ib) * SN + ia] = f | (ia == ib ? (1 << 30) : 0);
+              a.widx[(l * SN + ia) * SN + ib] = f | (ia == ib ? (1 << 30) : 0);
               a.ftab[f++] = fcode(j, jd, n, nd, l);
             }
         }
@@ -254,6 +264,7 @@ extern "C" int soapb_basis_plan(soapb_basis* b) {
   b->off_tab_b = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
   b->off_tab_bh = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
   b->off_ftab = off; off = align_up(off + 8 * (int64_t)b->n_feat_ps, 256);  // two int tables of F
+  b->off_widx = off; off = align_up(off + 4 * (int64_t)(L + 1) * (S * N) * (S * N), 256);
   b->off_err = off; off = align_up(off + 16, 256);
   b->bytes = off;
   b->dev = nullptr;
@@ -275,6 +286,7 @@ extern "C" int soapb_basis_build(soapb_basis* b, void* dev_buf, void* stream) {
   a.tab_b = (float*)(base + b->off_tab_b);
   a.tab_bh = (float*)(base + b->off_tab_bh);
   a.ftab = (int*)(base + b->off_ftab);
+  a.widx = (int*)(base + b->off_widx);
   a.err = (double*)(base + b->off_err);
   k_basis_build<<<1, 256, 0, (cudaStream_t)stream>>>(a);
   return check_launch("k_basis_build");

@@ -13,11 +13,19 @@
 //   F[neighbour] -= dE/drvec_e, and with attach F[centre atom] += dE/drvec_e
 //   (centres move with their atoms; self and own-image edges cancel).
 //
-// Mapping: one warp per centre (atomic work queue).  G is built in shared
-// memory; then, as in the descriptor kernel, lanes own radial functions
-// (n, l), pairs come sorted by (species, segment), solid harmonics and their
-// gradients are staged 32 edges at a time, and each edge's 3-vector is a
-// warp reduction followed by one atomic add per component.
+// Mapping: one warp per centre (atomic work queue), in two phases.
+//  1. G in shared memory: lane = a, loop over l and b; the feature of the pair
+//     {a, b} at l comes from a per-basis index table (bit 30 marks a = b), and
+//     dE/dp is gathered through the read-only cache.
+//  2. Edges in chunks of 32: lanes owning radial functions fn evaluate B_fn and
+//     Bhat_fn of the chunk's edges into shared memory (coefficients stay in
+//     registers while consecutive edges share a table segment, which the
+//     (species, segment) pair order makes the common case); then each lane
+//     contracts ONE edge: xi_lm = sum_n G[s, n, lm] B_nl, zeta_lm = sum_n
+//     G[s, n, lm] Bhat_nl, dE/drvec = sum_lm (rvec zeta_lm R_lm + xi_lm grad R_lm),
+//     with the solid harmonics of its own edge evaluated in registers, l by l.
+//     Neighbour forces are per-lane float atomics; the centre-atom force is
+//     accumulated in registers and reduced once per centre.
 #include "common.cuh"
 
 namespace soapb {
@@ -30,66 +38,62 @@ struct ForceArgs {
   const int* centre_atom;
   const float* tab_b;
   const float* tab_bh;
+  const int* widx;
   float* forces;
   int* counter;
   int64_t n_centres;
-  int N, S, nseg, F, crossover, attach;
+  int N, S, nseg, F, attach;
   float inv_h;
 };
-
-// Index of the power-spectrum feature of the unordered pair {(j,n), (jd,nd)} at l, or -1.
-__device__ __forceinline__ int feature_index(int j, int n, int jd, int nd, int l, int N, int S, int L, int crossover) {
-  if (j > jd || (j == jd && n > nd)) {
-    int t = j; j = jd; jd = t;
-    t = n; n = nd; nd = t;
-  }
-  const int Nd = N * (N + 1) / 2, No = N * N;
-  if (!crossover) {
-    if (j != jd) return -1;
-    return (j * Nd) * (L + 1) + l * Nd + (n * N - n * (n - 1) / 2 + (nd - n));
-  }
-  const int bi = j * S - j * (j - 1) / 2 + (jd - j);  // block index of (j, jd), j <= jd
-  const int ndiag = j + (jd > j ? 1 : 0);              // diagonal blocks before it
-  const int start = (ndiag * Nd + (bi - ndiag) * No) * (L + 1);
-  if (j == jd) return start + l * Nd + (n * N - n * (n - 1) / 2 + (nd - n));
-  return start + l * No + n * N + nd;
-}
 
 template <int L>
 struct ForceShape {
   static constexpr int K = (L + 1) * (L + 1);
   static constexpr int KC = K | 1;
-  static constexpr int YS = (4 * K) | 1;  // R and 3 gradient rows per staged edge
-  __host__ __device__ static int warp_floats(int S, int N, int F) { return 32 * YS + 128 + 2 * S * N * KC + F; }
+  static constexpr int RS = 33;  // staging row stride (floats): conflict-free lane and function strides
+  // per warp: G (S N KC) | union{ coefficients (S N KC), B and Bhat rows (2 N (L+1) RS) } | t, seg (64)
+  __host__ __device__ static int g_floats(int S, int N) { return (S * N * KC + 3) & ~3; }
+  __host__ __device__ static int u_floats(int S, int N) {
+    const int c = S * N * KC, st = 2 * N * (L + 1) * RS;
+    return ((c > st ? c : st) + 3) & ~3;
+  }
+  __host__ __device__ static int warp_floats(int S, int N) { return g_floats(S, N) + u_floats(S, N) + 64; }
 };
 
-template <int L, bool PAIRED>
+// Q_l^m table and the powers (x + i y)^m of one vector, for per-(l, m) solid
+// harmonics and gradients (same recurrences and normalisation as SolidHarmonics).
+template <int L>
+struct EdgeHarmonics {
+  static constexpr int NQ = (L + 1) * (L + 2) / 2;
+  float Q[NQ], C[L + 1], Sn[L + 1];
+  __device__ __forceinline__ EdgeHarmonics(float x, float y, float z) {
+    SolidHarmonics<L>::legendre(z, x * x + y * y + z * z, Q);
+    C[0] = 1.0f;
+    Sn[0] = 0.0f;
+#pragma unroll
+    for (int m = 1; m <= L; ++m) {
+      C[m] = x * C[m - 1] - y * Sn[m - 1];
+      Sn[m] = x * Sn[m - 1] + y * C[m - 1];
+    }
+  }
+};
+
+template <int L>
 __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
   using Sh = ForceShape<L>;
-  constexpr int K = Sh::K, KC = Sh::KC, YS = Sh::YS;
-  constexpr int MT = PAIRED ? 2 * L + 2 : 2 * L + 1;
-  extern __shared__ float sm[];
+  constexpr int K = Sh::K, KC = Sh::KC, RS = Sh::RS;
+  extern __shared__ __align__(16) float sm[];
   __shared__ float s_pref[kMaxL + 1];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int N = a.N, S = a.S, NF = N * (L + 1), F = a.F;
-  float* Y = sm + (size_t)wid * Sh::warp_floats(S, N, F);  // 32 x (R | dRx | dRy | dRz)
-  float* tt = Y + 32 * YS;
-  int* sg = (int*)(tt + 32);
-  int* spp = sg + 32;
-  int* atm = spp + 32;
-  float* cb = (float*)(atm + 32);  // S N KC coefficients
-  float* G = cb + S * N * KC;      // S N KC adjoint
-  float* w = G + S * N * KC;       // F
+  const int N = a.N, S = a.S, NF = N * (L + 1), SN = S * N, F = a.F;
+  float* G = sm + (size_t)wid * Sh::warp_floats(S, N);
+  float* U = G + Sh::g_floats(S, N);  // coefficients, then B / Bhat staging
+  float* Bs = U;
+  float* Hs = U + NF * RS;
+  float* s_t = U + Sh::u_floats(S, N);
+  int* s_seg = reinterpret_cast<int*>(s_t + 32);
   if (threadIdx.x <= L) s_pref[threadIdx.x] = sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * threadIdx.x + 1.0f));
   __syncthreads();
-
-  const LaneFns lf = lane_fns(lane, N, L, PAIRED);
-  const int m0 = lf.l0 >= 0 ? 2 * lf.l0 + 1 : 0;
-  const int mtot = m0 + (lf.l1 >= 0 ? 2 * lf.l1 + 1 : 0);
-  const int yoff0 = lf.l0 >= 0 ? lf.l0 * lf.l0 : 0;
-  const int yoff1 = lf.l1 >= 0 ? lf.l1 * lf.l1 - m0 : 0;
-  const int fn0 = lf.l0 >= 0 ? fn_index(lf.n0, lf.l0, N) : 0;
-  const int fn1 = lf.l1 >= 0 ? fn_index(lf.n1, lf.l1, N) : 0;
 
   for (;;) {
     int c32 = 0;
@@ -97,156 +101,191 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
     const int64_t c = __shfl_sync(0xffffffffu, c32, 0);
     if (c >= a.n_centres) break;
     const int catom = a.attach ? a.centre_atom[c] : -1;
-    for (int i = lane; i < S * N * K; i += 32) cb[(i / K) * KC + (i % K)] = a.coeff[(size_t)c * S * N * K + i];
-    for (int f = lane; f < F; f += 32) w[f] = a.dEdp[(size_t)c * F + f];
+    const float* crow = a.coeff + (size_t)c * SN * K;
+    for (int i = lane; i < SN * K; i += 32) U[(i / K) * KC + (i % K)] = crow[i];
     __syncwarp();
-    // G = dE/dc: one task per (a = (j, n), l)
-    for (int t = lane; t < S * N * (L + 1); t += 32) {
-      const int ai = t / (L + 1), l = t % (L + 1);
-      const int j = ai / N, n = ai % N;
-      float g[2 * L + 1];
+
+    // ---- G = dE/dc ----
+    const float* wrow = a.dEdp + (size_t)c * F;
+    for (int a0 = 0; a0 < SN; a0 += 32) {
+      const int ai = a0 + lane;
+      const bool act = ai < SN;
 #pragma unroll
-      for (int m = 0; m < 2 * L + 1; ++m) g[m] = 0.0f;
-      for (int bi = 0; bi < S * N; ++bi) {
-        const int f = feature_index(j, n, bi / N, bi % N, l, N, S, L, a.crossover);
-        if (f < 0) continue;
-        const float wt = w[f] * s_pref[l] * (bi == ai ? 2.0f : 1.0f);
-        const float* cr = cb + bi * KC + l * l;
+      for (int l = 0; l <= L; ++l) {
+        float g[2 * L + 1];
 #pragma unroll
-        for (int m = 0; m < 2 * L + 1; ++m)
-          if (m < 2 * l + 1) g[m] = fmaf(wt, cr[m], g[m]);
+        for (int m = 0; m < 2 * L + 1; ++m) g[m] = 0.0f;
+        const int* wl = a.widx + (size_t)l * SN * SN;
+        for (int bi = 0; bi < SN; ++bi) {
+          const int code = act ? __ldg(wl + (size_t)bi * SN + ai) : -1;
+          if (code >= 0) {
+            float w = __ldg(wrow + (code & 0x3fffffff));
+            if (code & (1 << 30)) w *= 2.0f;
+            const float* cr = U + bi * KC + l * l;
+#pragma unroll
+            for (int m = 0; m < 2 * l + 1; ++m) g[m] = fmaf(w, cr[m], g[m]);
+          }
+        }
+        if (act) {
+#pragma unroll
+          for (int m = 0; m < 2 * l + 1; ++m) G[ai * KC + l * l + m] = s_pref[l] * g[m];
+        }
       }
-#pragma unroll
-      for (int m = 0; m < 2 * L + 1; ++m)
-        if (m < 2 * l + 1) G[ai * KC + l * l + m] = g[m];
     }
     __syncwarp();
 
-    float gr[MT];
-    float cf0[kNCoef], cf1[kNCoef], ch0[kNCoef], ch1[kNCoef];
-#pragma unroll
-    for (int k = 0; k < kNCoef; ++k) { cf0[k] = cf1[k] = ch0[k] = ch1[k] = 0.0f; }
-#pragma unroll
-    for (int k = 0; k < MT; ++k) gr[k] = 0.0f;
-    int cur_sp = -1, cur_seg = -1;
-    float fcx = 0.f, fcy = 0.f, fcz = 0.f;  // centre-atom force (lane 0)
+    // ---- edges ----
+    float fcx = 0.f, fcy = 0.f, fcz = 0.f;
     const int64_t p0 = a.pair_off[c], p1 = a.pair_off[c + 1];
     for (int64_t base = p0; base < p1; base += 32) {
       const int nt = (int)min((int64_t)32, p1 - base);
+      float4 pr = make_float4(0.f, 0.f, 0.f, 0.f);
       if (lane < nt) {
-        const float4 pr = __ldg(a.pairs + base + lane);
-        const int wd = __float_as_int(pr.w);
+        pr = __ldg(a.pairs + base + lane);
         const float r = sqrtf(pr.x * pr.x + pr.y * pr.y + pr.z * pr.z);
         int seg;
         float t;
         seg_coord(r, a.inv_h, a.nseg, seg, t);
-        tt[lane] = t;
-        sg[lane] = seg;
-        spp[lane] = (int)((unsigned)wd >> kAtomBits);
-        atm[lane] = wd & kAtomMask;
-        float* yrow = Y + lane * YS;
-        SolidHarmonics<L>::with_gradients(pr.x, pr.y, pr.z, [&](int idx, float v, float dx, float dy, float dz) {
-          yrow[idx] = v; yrow[K + idx] = dx; yrow[2 * K + idx] = dy; yrow[3 * K + idx] = dz;
-        });
+        s_t[lane] = t;
+        s_seg[lane] = seg;
       }
       __syncwarp();
-      for (int q = 0; q < nt; ++q) {
-        const int sp = spp[q];
-        if (sp != cur_sp) {
+      // radial functions of the chunk: lane owns fn, lane + 32, ...
+      for (int fn = lane; fn < NF; fn += 32) {
+        float cf[kNCoef], ch[kNCoef];
+        int cur = -1;
+        for (int q = 0; q < nt; ++q) {
+          const int sq = s_seg[q];
+          if (sq != cur) {
+            load_coef(a.tab_b, sq, fn, NF, cf);
+            load_coef(a.tab_bh, sq, fn, NF, ch);
+            cur = sq;
+          }
+          const float tq = s_t[q];
+          Bs[fn * RS + q] = horner7(cf, tq);
+          Hs[fn * RS + q] = horner7(ch, tq);
+        }
+      }
+      __syncwarp();
+      if (lane < nt) {
+        const int wd = __float_as_int(pr.w);
+        const int sp = (int)((unsigned)wd >> kAtomBits), atom = wd & kAtomMask;
+        const float x = pr.x, y = pr.y, z = pr.z;
+        const EdgeHarmonics<L> eh(x, y, z);
+        const float* gs = G + sp * N * KC;
+        float ex = 0.f, ey = 0.f, ez = 0.f;
 #pragma unroll
-          for (int k = 0; k < MT; ++k) {
-            gr[k] = 0.0f;
-            if (k < mtot) {
-              const bool first = k < m0;
-              const int n = first ? lf.n0 : lf.n1, l = first ? lf.l0 : lf.l1, m = first ? k : k - m0;
-              gr[k] = G[(sp * N + n) * KC + l * l + m];
+        for (int l = 0; l <= L; ++l) {
+          float xi[2 * L + 1], ze[2 * L + 1];
+#pragma unroll
+          for (int m = 0; m < 2 * l + 1; ++m) { xi[m] = 0.0f; ze[m] = 0.0f; }
+          for (int n = 0; n < N; ++n) {
+            const float b = Bs[(l * N + n) * RS + lane], h = Hs[(l * N + n) * RS + lane];
+            const float* gr = gs + n * KC + l * l;
+#pragma unroll
+            for (int m = 0; m < 2 * l + 1; ++m) {
+              const float gv = gr[m];
+              xi[m] = fmaf(gv, b, xi[m]);
+              ze[m] = fmaf(gv, h, ze[m]);
             }
           }
-          cur_sp = sp;
-        }
-        const int seg = sg[q];
-        if (seg != cur_seg) {
-          if (lf.l0 >= 0) { load_coef(a.tab_b, seg, fn0, NF, cf0); load_coef(a.tab_bh, seg, fn0, NF, ch0); }
-          if (PAIRED && lf.l1 >= 0) { load_coef(a.tab_b, seg, fn1, NF, cf1); load_coef(a.tab_bh, seg, fn1, NF, ch1); }
-          cur_seg = seg;
-        }
-        const float t = tt[q];
-        const float B0 = horner7(cf0, t), H0 = horner7(ch0, t);
-        const float B1 = PAIRED ? horner7(cf1, t) : 0.0f, H1 = PAIRED ? horner7(ch1, t) : 0.0f;
-        const float* yr = Y + q * YS;
-        float u0 = 0.f, u1 = 0.f, vx0 = 0.f, vx1 = 0.f, vy0 = 0.f, vy1 = 0.f, vz0 = 0.f, vz1 = 0.f;
+          // solid harmonics R_l^m and gradients (index l + m within the l block)
 #pragma unroll
-        for (int k = 0; k < MT; ++k) {
-          if (k < mtot) {
-            const bool first = k < m0;
-            const int yi = k + (first ? yoff0 : yoff1);
-            const float g = gr[k];
-            const float ru = g * yr[yi], rx = g * yr[K + yi], ry = g * yr[2 * K + yi], rz = g * yr[3 * K + yi];
-            if (first) { u0 += ru; vx0 += rx; vy0 += ry; vz0 += rz; }
-            else { u1 += ru; vx1 += rx; vy1 += ry; vz1 += rz; }
+          for (int m = 0; m <= l; ++m) {
+            const float nrm = c_shnorm[l * (kMaxL + 1) + m];
+            const float q = eh.Q[tri(l, m)];
+            const float qp = (l >= 1 && m + 1 <= l - 1) ? eh.Q[tri(l - 1, m + 1)] : 0.0f;
+            const float qz = (l >= 1 && m <= l - 1) ? (float)(l + m) * eh.Q[tri(l - 1, m)] : 0.0f;
+            if (m == 0) {
+              const float R = nrm * q, dx = nrm * (-x * qp), dy = nrm * (-y * qp), dz = nrm * qz;
+              const float zr = ze[l] * R;
+              ex += x * zr + xi[l] * dx;
+              ey += y * zr + xi[l] * dy;
+              ez += z * zr + xi[l] * dz;
+            } else {
+              const float fm = (float)m;
+              const float Cm = eh.C[m], Sm = eh.Sn[m], Cp = eh.C[m - 1], Sp = eh.Sn[m - 1];
+              {  // +m
+                const float R = nrm * q * Cm;
+                const float dx = nrm * (-x * qp * Cm + q * fm * Cp), dy = nrm * (-y * qp * Cm - q * fm * Sp);
+                const float dz = nrm * qz * Cm;
+                const float zr = ze[l + m] * R;
+                ex += x * zr + xi[l + m] * dx;
+                ey += y * zr + xi[l + m] * dy;
+                ez += z * zr + xi[l + m] * dz;
+              }
+              {  // -m
+                const float R = nrm * q * Sm;
+                const float dx = nrm * (-x * qp * Sm + q * fm * Sp), dy = nrm * (-y * qp * Sm + q * fm * Cp);
+                const float dz = nrm * qz * Sm;
+                const float zr = ze[l - m] * R;
+                ex += x * zr + xi[l - m] * dx;
+                ey += y * zr + xi[l - m] * dy;
+                ez += z * zr + xi[l - m] * dz;
+              }
+            }
           }
         }
-        // rvec from the pair (re-read: rows hold R and gradients only)
-        const float4 pr = __ldg(a.pairs + base + q);
-        const float hu = H0 * u0 + H1 * u1;
-        float ex = pr.x * hu + B0 * vx0 + B1 * vx1;
-        float ey = pr.y * hu + B0 * vy0 + B1 * vy1;
-        float ez = pr.z * hu + B0 * vz0 + B1 * vz1;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          ex += __shfl_xor_sync(0xffffffffu, ex, o);
-          ey += __shfl_xor_sync(0xffffffffu, ey, o);
-          ez += __shfl_xor_sync(0xffffffffu, ez, o);
-        }
-        const int atom = atm[q];
-        if (lane == 0) {
-          if (!(a.attach && atom == catom)) {
-            atomicAdd(&a.forces[3 * (size_t)atom + 0], -ex);
-            atomicAdd(&a.forces[3 * (size_t)atom + 1], -ey);
-            atomicAdd(&a.forces[3 * (size_t)atom + 2], -ez);
-            fcx += ex; fcy += ey; fcz += ez;
-          }
+        if (!(a.attach && atom == catom)) {
+          atomicAdd(&a.forces[3 * (size_t)atom + 0], -ex);
+          atomicAdd(&a.forces[3 * (size_t)atom + 1], -ey);
+          atomicAdd(&a.forces[3 * (size_t)atom + 2], -ez);
+          fcx += ex;
+          fcy += ey;
+          fcz += ez;
         }
       }
       __syncwarp();
     }
-    if (lane == 0 && catom >= 0) {
-      atomicAdd(&a.forces[3 * (size_t)catom + 0], fcx);
-      atomicAdd(&a.forces[3 * (size_t)catom + 1], fcy);
-      atomicAdd(&a.forces[3 * (size_t)catom + 2], fcz);
+    if (catom >= 0) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        fcx += __shfl_xor_sync(0xffffffffu, fcx, o);
+        fcy += __shfl_xor_sync(0xffffffffu, fcy, o);
+        fcz += __shfl_xor_sync(0xffffffffu, fcz, o);
+      }
+      if (lane == 0) {
+        atomicAdd(&a.forces[3 * (size_t)catom + 0], fcx);
+        atomicAdd(&a.forces[3 * (size_t)catom + 1], fcy);
+        atomicAdd(&a.forces[3 * (size_t)catom + 2], fcz);
+      }
     }
     __syncwarp();
   }
 }
 
-template <int L, bool PAIRED>
-static int launch_forces(const ForceArgs& a, cudaStream_t st) {
-  const int per_warp = 4 * ForceShape<L>::warp_floats(a.S, a.N, a.F);
-  int wpb = (200 * 1024) / per_warp;
-  wpb = wpb > 4 ? 4 : wpb;
-  if (wpb < 1) return set_error(SOAPB_ERR_UNSUPPORTED, "forces shared memory %d B per warp too large", per_warp);
-  const int smem = wpb * per_warp;
-  auto kern = k_forces<L, PAIRED>;
-  int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
-                      "forces smem attribute");
-  if (rc) return rc;
-  int dev = 0, nsm = 148, occ = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 * wpb, smem);
-  if (occ < 1) occ = 1;
-  int64_t blocks = (int64_t)nsm * occ;
-  const int64_t need = (a.n_centres + wpb - 1) / wpb;
-  if (blocks > need) blocks = need;
-  if (blocks < 1) blocks = 1;
-  kern<<<(unsigned)blocks, 32 * wpb, smem, st>>>(a);
-  return check_launch("k_forces");
-}
-
 template <int L>
 struct ForceDispatch {
-  static int run(const ForceArgs& a, bool paired, cudaStream_t st) {
-    return paired ? launch_forces<L, true>(a, st) : launch_forces<L, false>(a, st);
+  static int run(const ForceArgs& a, cudaStream_t st) {
+    auto kern = k_forces<L>;
+    const int per_warp = 4 * ForceShape<L>::warp_floats(a.S, a.N);
+    int dev = 0, nsm = 148, smem_sm = 228 * 1024, smem_blk = 227 * 1024;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    // warps per block: the most resident warps per SM (1 KB reserved per block), larger blocks on ties
+    int wpb = 0, best = 0;
+    for (int w = 4; w >= 1; w >>= 1) {
+      const int bytes = w * per_warp;
+      if (bytes > smem_blk) continue;
+      const int resident = w * (smem_sm / (bytes + 1024));
+      if (resident > best) { best = resident; wpb = w; }
+    }
+    if (wpb == 0) return set_error(SOAPB_ERR_UNSUPPORTED, "forces shared memory %d B per warp too large", per_warp);
+    const int smem = wpb * per_warp;
+    int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                        "forces smem attribute");
+    if (rc) return rc;
+    int occ = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 * wpb, smem);
+    if (occ < 1) occ = 1;
+    int64_t blocks = (int64_t)nsm * occ;
+    const int64_t need = (a.n_centres + wpb - 1) / wpb;
+    if (blocks > need) blocks = need;
+    if (blocks < 1) blocks = 1;
+    kern<<<(unsigned)blocks, 32 * wpb, smem, st>>>(a);
+    return check_launch("k_forces");
   }
 };
 
@@ -263,10 +302,6 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   if (!d_pair_off || !d_coeff || !d_dEdp || !d_forces || !d_counter) return set_error(SOAPB_ERR_ARG, "null argument");
   if (attach && !d_centre_atom) return set_error(SOAPB_ERR_ARG, "attach needs centre atoms");
   const int N = b->n_max, L = b->l_max;
-  bool paired;
-  if (N * (L + 1) <= 32) paired = false;
-  else if (lanes_needed(N, L, true) <= 32) paired = true;
-  else return set_error(SOAPB_ERR_UNSUPPORTED, "n_max * (l_max + 1) = %d radial functions exceed one warp", N * (L + 1));
   cudaStream_t st = (cudaStream_t)stream;
   ForceArgs a;
   a.pair_off = d_pair_off;
@@ -276,6 +311,7 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.centre_atom = d_centre_atom;
   a.tab_b = (const float*)((const char*)b->dev + b->off_tab_b);
   a.tab_bh = (const float*)((const char*)b->dev + b->off_tab_bh);
+  a.widx = (const int*)((const char*)b->dev + b->off_widx);
   a.forces = d_forces;
   a.counter = d_counter;
   a.n_centres = n_centres;
@@ -283,10 +319,9 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.S = b->n_species;
   a.nseg = b->n_seg;
   a.F = b->n_feat_ps;
-  a.crossover = b->crossover ? 1 : 0;
   a.attach = attach ? 1 : 0;
   a.inv_h = (float)(1.0 / b->seg_width);
   int rc = check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st), "reset work counter");
   if (rc) return rc;
-  return dispatch_l<ForceDispatch>(L, a, paired, st);
+  return dispatch_l<ForceDispatch>(L, a, st);
 }

@@ -67,7 +67,7 @@ typedef struct soapb_basis {
   int32_t n_feat_ps; /* SG:913-919 */
   int32_t n_feat_cc; /* SG:909-910 */
   int64_t bytes;     /* device bytes the basis needs */
-  int64_t off_alpha, off_beta, off_tab_b, off_tab_bh, off_ftab, off_err;  /* byte offsets into dev */
+  int64_t off_alpha, off_beta, off_tab_b, off_tab_bh, off_ftab, off_widx, off_err;  /* byte offsets into dev */
   void* dev;         /* set by soapb_basis_build */
 } soapb_basis;
 
