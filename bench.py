@@ -248,6 +248,42 @@ def batched_vs_plain(soap_cls, torch):
             "speedup": res["batched"] / res["plain"]}
 
 
+def run_batched_only(args):
+    """--batched-cells K: the batched path alone (descriptor + adjoint forces
+    of E = sum w.p) on the first K cells of the 512-cell workload, one warm-up
+    and --steps timed passes, with per-stage CUDA-event times; a profiling
+    case for the batched kernels (prints one JSON line, not a bench value)."""
+    import torch
+    from cusoap_b200 import SOAP, workloads as W
+    torch.cuda.set_device(0)
+    cells = W.make("cells512")[:args.batched_cells]
+    soap = SOAP(**W.CONFIGS["cells512"])
+    rng = np.random.default_rng(0)
+    w = torch.tensor(rng.standard_normal(soap.get_number_of_features()), dtype=torch.float32, device="cuda")
+    dev_cells = [{"positions": torch.tensor(c["positions"], device="cuda"), "atomic_numbers": c["atomic_numbers"],
+                  "cell": c["cell"], "pbc": c["pbc"]} for c in cells]
+
+    def one():
+        sysl = [dict(c, positions=c["positions"].clone().requires_grad_(True)) for c in dev_cells]
+        out = soap.create(sysl)
+        E = sum((o * w).sum() for o in out) if isinstance(out, list) else (out * w).sum()
+        E.backward()
+
+    one()
+    torch.cuda.synchronize()
+    soap.profile = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        one()
+    e1.record()
+    torch.cuda.synchronize()
+    st = {k: v / args.steps for k, v in soap.stage_times().items()}
+    n_atoms = sum(len(c["atomic_numbers"]) for c in cells)
+    print(json.dumps({"workload": f"first {len(cells)} cells of the 512-cell batch ({n_atoms} atoms)",
+                      "ms_per_step": e0.elapsed_time(e1) / args.steps, "stage_ms_per_step": st}), flush=True)
+
+
 def run_ours(args):
     import torch
     world, rank, local = _dist()
@@ -390,8 +426,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-cells", type=int, default=0,
+                    help="profiling case: run only the batched path on the first K cells")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.batched_cells > 0:
+        run_batched_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

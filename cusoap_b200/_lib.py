@@ -20,7 +20,7 @@ EXPORTS = (
     "soapb_basis_plan", "soapb_basis_build", "soapb_basis_download",
     "soapb_neighbors_workspace", "soapb_neighbors_count", "soapb_neighbors_fill", "soapb_neighbors_status",
     "soapb_neighbors_stats", "soapb_neighbors_noalloc",
-    "soapb_descriptor", "soapb_jacobian_workspace", "soapb_jacobian", "soapb_forces",
+    "soapb_descriptor", "soapb_jacobian_workspace", "soapb_jacobian", "soapb_forces_workspace", "soapb_forces",
     "soapb_last_error", "soapb_version", "soapb_kernel_launches",
 )
 
@@ -34,6 +34,7 @@ class Basis(ctypes.Structure):
         ("bytes", c_int64),
         ("off_alpha", c_int64), ("off_beta", c_int64), ("off_tab_b", c_int64), ("off_tab_bh", c_int64),
         ("off_ftab", c_int64), ("off_widx", c_int64), ("off_err", c_int64),
+        ("off_tabt_b", c_int64), ("off_tabt_bh", c_int64),
         ("dev", c_void_p),
     ]
 
@@ -85,7 +86,8 @@ def load() -> ctypes.CDLL:
         "soapb_jacobian_workspace": [POINTER(Basis), c_int64, c_int64, c_int64, c_int32, POINTER(c_int64)],
         "soapb_jacobian": [POINTER(Basis), c_int64, P, P, c_int64, P, P, c_int64, P, c_int32, c_int32, c_int32, P,
                            P, c_int64, P, P],
-        "soapb_forces": [POINTER(Basis), c_int64, P, P, P, P, P, c_int32, P, P, P],
+        "soapb_forces_workspace": [POINTER(Basis), c_int64, POINTER(c_int64)],
+        "soapb_forces": [POINTER(Basis), c_int64, P, P, P, P, P, c_int32, P, P, c_int64, P, P],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

@@ -29,6 +29,8 @@ struct BasisDev {
   double* beta;
   float* tab_b;
   float* tab_bh;
+  float* tabt_b;   // function-major copies: [fn][seg][8]
+  float* tabt_bh;
   int* ftab;
   int* widx;
   double* err;
@@ -152,7 +154,8 @@ __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
         for (int k = 0; k < kNCoef; ++k) { Tprev[k] = Tcur[k]; Tcur[k] = Tnext[k]; }
       }
       float* dst = (which ? a.tab_bh : a.tab_b) + ((size_t)seg * NF + fn) * kNCoef;
-      for (int k = 0; k < kNCoef; ++k) dst[k] = (float)mono[k];
+      float* dstt = (which ? a.tabt_bh : a.tabt_b) + ((size_t)fn * a.nseg + seg) * kNCoef;
+      for (int k = 0; k < kNCoef; ++k) dst[k] = dstt[k] = (float)mono[k];
     }
   }
   if (tid == 0) { a.err[0] = 0.0; a.err[1] = 0.0; }
@@ -266,6 +269,8 @@ extern "C" int soapb_basis_plan(soapb_basis* b) {
   b->off_ftab = off; off = align_up(off + 8 * (int64_t)b->n_feat_ps, 256);  // two int tables of F
   b->off_widx = off; off = align_up(off + 4 * (int64_t)(L + 1) * (S * N) * (S * N), 256);
   b->off_err = off; off = align_up(off + 16, 256);
+  b->off_tabt_b = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
+  b->off_tabt_bh = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
   b->bytes = off;
   b->dev = nullptr;
   return SOAPB_OK;
@@ -285,6 +290,8 @@ extern "C" int soapb_basis_build(soapb_basis* b, void* dev_buf, void* stream) {
   a.beta = (double*)(base + b->off_beta);
   a.tab_b = (float*)(base + b->off_tab_b);
   a.tab_bh = (float*)(base + b->off_tab_bh);
+  a.tabt_b = (float*)(base + b->off_tabt_b);
+  a.tabt_bh = (float*)(base + b->off_tabt_bh);
   a.ftab = (int*)(base + b->off_ftab);
   a.widx = (int*)(base + b->off_widx);
   a.err = (double*)(base + b->off_err);

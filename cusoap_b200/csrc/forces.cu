@@ -13,19 +13,21 @@
 //   F[neighbour] -= dE/drvec_e, and with attach F[centre atom] += dE/drvec_e
 //   (centres move with their atoms; self and own-image edges cancel).
 //
-// Mapping: one warp per centre (atomic work queue), in two phases.
-//  1. G in shared memory: lane = a, loop over l and b; the feature of the pair
-//     {a, b} at l comes from a per-basis index table (bit 30 marks a = b), and
-//     dE/dp is gathered through the read-only cache.
-//  2. Edges in chunks of 32: lanes owning radial functions fn evaluate B_fn and
-//     Bhat_fn of the chunk's edges into shared memory (coefficients stay in
-//     registers while consecutive edges share a table segment, which the
-//     (species, segment) pair order makes the common case); then each lane
-//     contracts ONE edge: xi_lm = sum_n G[s, n, lm] B_nl, zeta_lm = sum_n
-//     G[s, n, lm] Bhat_nl, dE/drvec = sum_lm (rvec zeta_lm R_lm + xi_lm grad R_lm),
-//     with the solid harmonics of its own edge evaluated in registers, l by l.
-//     Neighbour forces are per-lane float atomics; the centre-atom force is
-//     accumulated in registers and reduced once per centre.
+// Two kernels:
+//  k_adjoint_g  one block per centre: dE/dp row and coefficient row staged in
+//               shared memory (coalesced), G[a, lm] computed by thread-tasks
+//               (a, l); the pair {a, b} -> feature map is a per-basis index
+//               table (bit 30 marks a = b).  G goes to the workspace.
+//  k_forces     one warp per centre (atomic work queue), ONE edge per lane:
+//               the lane evaluates its edge's radial functions B_nl, Bhat_nl
+//               from the function-major copy of the tables (lanes on nearby
+//               segments share cache lines), its solid harmonics in registers,
+//               and contracts l by l:
+//                 xi_lm = sum_n G[s, n, lm] B_nl, zeta_lm = sum_n G[s, n, lm] Bhat_nl,
+//                 dE/drvec = sum_lm (rvec zeta_lm R_lm + xi_lm grad R_lm),
+//               with G broadcast from shared memory.  Neighbour forces are
+//               per-lane float atomics; the centre-atom force is accumulated
+//               in registers and reduced once per centre.
 #include "common.cuh"
 
 namespace soapb {
@@ -36,9 +38,10 @@ struct ForceArgs {
   const float* coeff;
   const float* dEdp;
   const int* centre_atom;
-  const float* tab_b;
-  const float* tab_bh;
+  const float* tabt_b;   // [fn][seg][8]
+  const float* tabt_bh;
   const int* widx;
+  float* G;              // (n_centres, S N K) workspace
   float* forces;
   int* counter;
   int64_t n_centres;
@@ -46,19 +49,51 @@ struct ForceArgs {
   float inv_h;
 };
 
-template <int L>
-struct ForceShape {
-  static constexpr int K = (L + 1) * (L + 1);
-  static constexpr int KC = K | 1;
-  static constexpr int RS = 33;  // staging row stride (floats): conflict-free lane and function strides
-  // per warp: G (S N KC) | union{ coefficients (S N KC), B and Bhat rows (2 N (L+1) RS) } | t, seg (64)
-  __host__ __device__ static int g_floats(int S, int N) { return (S * N * KC + 3) & ~3; }
-  __host__ __device__ static int u_floats(int S, int N) {
-    const int c = S * N * KC, st = 2 * N * (L + 1) * RS;
-    return ((c > st ? c : st) + 3) & ~3;
+constexpr int kGThreads = 256;
+
+// G = dE/dc for one centre per block iteration.  STAGE_W: the dE/dp row is
+// staged in shared memory (else read through the read-only cache, for
+// feature counts whose row does not fit).
+template <int L, bool STAGE_W>
+__global__ void __launch_bounds__(kGThreads) k_adjoint_g(ForceArgs a) {
+  constexpr int K = (L + 1) * (L + 1), KC = K | 1;
+  extern __shared__ __align__(16) float sm[];
+  const int N = a.N, SN = a.S * N, F = a.F;
+  float* s_c = sm;                                   // SN x KC
+  float* s_w = sm + ((SN * KC + 3) & ~3);            // F (STAGE_W)
+  for (int64_t c = blockIdx.x; c < a.n_centres; c += gridDim.x) {
+    const float* wrow = a.dEdp + (size_t)c * F;
+    const float* crow = a.coeff + (size_t)c * SN * K;
+    if (STAGE_W)
+      for (int f = threadIdx.x; f < F; f += blockDim.x) s_w[f] = wrow[f];
+    for (int i = threadIdx.x; i < SN * K; i += blockDim.x) s_c[(i / K) * KC + (i % K)] = crow[i];
+    __syncthreads();
+    float* grow = a.G + (size_t)c * SN * K;
+    // tasks (a, l), heaviest l first so the last round is light
+    for (int t = threadIdx.x; t < SN * (L + 1); t += blockDim.x) {
+      const int l = L - t / SN, ai = t % SN;
+      const int* wl = a.widx + (size_t)l * SN * SN;
+      float g[2 * L + 1];
+#pragma unroll
+      for (int m = 0; m < 2 * L + 1; ++m) g[m] = 0.0f;
+      for (int bi = 0; bi < SN; ++bi) {
+        const int code = __ldg(wl + (size_t)bi * SN + ai);
+        if (code < 0) continue;
+        const int f = code & 0x3fffffff;
+        const float w = (STAGE_W ? s_w[f] : __ldg(wrow + f)) * ((code & (1 << 30)) ? 2.0f : 1.0f);
+        const float* cr = s_c + bi * KC + l * l;
+#pragma unroll
+        for (int m = 0; m < 2 * L + 1; ++m)
+          if (m < 2 * l + 1) g[m] = fmaf(w, cr[m], g[m]);
+      }
+      const float pref = sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * l + 1.0f));
+#pragma unroll
+      for (int m = 0; m < 2 * L + 1; ++m)
+        if (m < 2 * l + 1) grow[ai * K + l * l + m] = pref * g[m];
+    }
+    __syncthreads();
   }
-  __host__ __device__ static int warp_floats(int S, int N) { return g_floats(S, N) + u_floats(S, N) + 64; }
-};
+}
 
 // Q_l^m table and the powers (x + i y)^m of one vector, for per-(l, m) solid
 // harmonics and gradients (same recurrences and normalisation as SolidHarmonics).
@@ -79,21 +114,20 @@ struct EdgeHarmonics {
 };
 
 template <int L>
+struct ForceShape {
+  static constexpr int K = (L + 1) * (L + 1);
+  static constexpr int KC = K | 1;
+  __host__ __device__ static int warp_floats(int S, int N) { return (S * N * KC + 3) & ~3; }
+};
+
+template <int L>
 __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
   using Sh = ForceShape<L>;
-  constexpr int K = Sh::K, KC = Sh::KC, RS = Sh::RS;
+  constexpr int K = Sh::K, KC = Sh::KC;
   extern __shared__ __align__(16) float sm[];
-  __shared__ float s_pref[kMaxL + 1];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int N = a.N, S = a.S, NF = N * (L + 1), SN = S * N, F = a.F;
-  float* G = sm + (size_t)wid * Sh::warp_floats(S, N);
-  float* U = G + Sh::g_floats(S, N);  // coefficients, then B / Bhat staging
-  float* Bs = U;
-  float* Hs = U + NF * RS;
-  float* s_t = U + Sh::u_floats(S, N);
-  int* s_seg = reinterpret_cast<int*>(s_t + 32);
-  if (threadIdx.x <= L) s_pref[threadIdx.x] = sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * threadIdx.x + 1.0f));
-  __syncthreads();
+  const int N = a.N, SN = a.S * N, nseg = a.nseg;
+  float* G = sm + (size_t)wid * Sh::warp_floats(a.S, N);
 
   for (;;) {
     int c32 = 0;
@@ -101,141 +135,87 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
     const int64_t c = __shfl_sync(0xffffffffu, c32, 0);
     if (c >= a.n_centres) break;
     const int catom = a.attach ? a.centre_atom[c] : -1;
-    const float* crow = a.coeff + (size_t)c * SN * K;
-    for (int i = lane; i < SN * K; i += 32) U[(i / K) * KC + (i % K)] = crow[i];
+    const float* grow = a.G + (size_t)c * SN * K;
+    for (int i = lane; i < SN * K; i += 32) G[(i / K) * KC + (i % K)] = grow[i];
     __syncwarp();
 
-    // ---- G = dE/dc ----
-    const float* wrow = a.dEdp + (size_t)c * F;
-    for (int a0 = 0; a0 < SN; a0 += 32) {
-      const int ai = a0 + lane;
-      const bool act = ai < SN;
-#pragma unroll
-      for (int l = 0; l <= L; ++l) {
-        float g[2 * L + 1];
-#pragma unroll
-        for (int m = 0; m < 2 * L + 1; ++m) g[m] = 0.0f;
-        const int* wl = a.widx + (size_t)l * SN * SN;
-        for (int bi = 0; bi < SN; ++bi) {
-          const int code = act ? __ldg(wl + (size_t)bi * SN + ai) : -1;
-          if (code >= 0) {
-            float w = __ldg(wrow + (code & 0x3fffffff));
-            if (code & (1 << 30)) w *= 2.0f;
-            const float* cr = U + bi * KC + l * l;
-#pragma unroll
-            for (int m = 0; m < 2 * l + 1; ++m) g[m] = fmaf(w, cr[m], g[m]);
-          }
-        }
-        if (act) {
-#pragma unroll
-          for (int m = 0; m < 2 * l + 1; ++m) G[ai * KC + l * l + m] = s_pref[l] * g[m];
-        }
-      }
-    }
-    __syncwarp();
-
-    // ---- edges ----
     float fcx = 0.f, fcy = 0.f, fcz = 0.f;
     const int64_t p0 = a.pair_off[c], p1 = a.pair_off[c + 1];
-    for (int64_t base = p0; base < p1; base += 32) {
-      const int nt = (int)min((int64_t)32, p1 - base);
-      float4 pr = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (lane < nt) {
-        pr = __ldg(a.pairs + base + lane);
-        const float r = sqrtf(pr.x * pr.x + pr.y * pr.y + pr.z * pr.z);
-        int seg;
-        float t;
-        seg_coord(r, a.inv_h, a.nseg, seg, t);
-        s_t[lane] = t;
-        s_seg[lane] = seg;
-      }
-      __syncwarp();
-      // radial functions of the chunk: lane owns fn, lane + 32, ...
-      for (int fn = lane; fn < NF; fn += 32) {
-        float cf[kNCoef], ch[kNCoef];
-        int cur = -1;
-        for (int q = 0; q < nt; ++q) {
-          const int sq = s_seg[q];
-          if (sq != cur) {
-            load_coef(a.tab_b, sq, fn, NF, cf);
-            load_coef(a.tab_bh, sq, fn, NF, ch);
-            cur = sq;
+    for (int64_t e = p0 + lane; e < p1; e += 32) {
+      const float4 pr = __ldg(a.pairs + e);
+      const int wd = __float_as_int(pr.w);
+      const int sp = (int)((unsigned)wd >> kAtomBits), atom = wd & kAtomMask;
+      const float x = pr.x, y = pr.y, z = pr.z;
+      int seg;
+      float t;
+      seg_coord(sqrtf(x * x + y * y + z * z), a.inv_h, nseg, seg, t);
+      const EdgeHarmonics<L> eh(x, y, z);
+      const float* gs = G + sp * N * KC;
+      float ex = 0.f, ey = 0.f, ez = 0.f;
+#pragma unroll
+      for (int l = 0; l <= L; ++l) {
+        float xi[2 * L + 1], ze[2 * L + 1];
+#pragma unroll
+        for (int m = 0; m < 2 * l + 1; ++m) { xi[m] = 0.0f; ze[m] = 0.0f; }
+        for (int n = 0; n < N; ++n) {
+          const int fn = l * N + n;
+          float cf[kNCoef], ch[kNCoef];
+          load_coef(a.tabt_b, fn, seg, nseg, cf);   // function-major: row fn, column seg
+          load_coef(a.tabt_bh, fn, seg, nseg, ch);
+          const float b = horner7(cf, t), h = horner7(ch, t);
+          const float* gr = gs + n * KC + l * l;
+#pragma unroll
+          for (int m = 0; m < 2 * l + 1; ++m) {
+            const float gv = gr[m];
+            xi[m] = fmaf(gv, b, xi[m]);
+            ze[m] = fmaf(gv, h, ze[m]);
           }
-          const float tq = s_t[q];
-          Bs[fn * RS + q] = horner7(cf, tq);
-          Hs[fn * RS + q] = horner7(ch, tq);
         }
-      }
-      __syncwarp();
-      if (lane < nt) {
-        const int wd = __float_as_int(pr.w);
-        const int sp = (int)((unsigned)wd >> kAtomBits), atom = wd & kAtomMask;
-        const float x = pr.x, y = pr.y, z = pr.z;
-        const EdgeHarmonics<L> eh(x, y, z);
-        const float* gs = G + sp * N * KC;
-        float ex = 0.f, ey = 0.f, ez = 0.f;
+        // solid harmonics R_l^m and gradients (index l + m within the l block)
 #pragma unroll
-        for (int l = 0; l <= L; ++l) {
-          float xi[2 * L + 1], ze[2 * L + 1];
-#pragma unroll
-          for (int m = 0; m < 2 * l + 1; ++m) { xi[m] = 0.0f; ze[m] = 0.0f; }
-          for (int n = 0; n < N; ++n) {
-            const float b = Bs[(l * N + n) * RS + lane], h = Hs[(l * N + n) * RS + lane];
-            const float* gr = gs + n * KC + l * l;
-#pragma unroll
-            for (int m = 0; m < 2 * l + 1; ++m) {
-              const float gv = gr[m];
-              xi[m] = fmaf(gv, b, xi[m]);
-              ze[m] = fmaf(gv, h, ze[m]);
+        for (int m = 0; m <= l; ++m) {
+          const float nrm = c_shnorm[l * (kMaxL + 1) + m];
+          const float q = eh.Q[tri(l, m)];
+          const float qp = (l >= 1 && m + 1 <= l - 1) ? eh.Q[tri(l - 1, m + 1)] : 0.0f;
+          const float qz = (l >= 1 && m <= l - 1) ? (float)(l + m) * eh.Q[tri(l - 1, m)] : 0.0f;
+          if (m == 0) {
+            const float R = nrm * q, dx = nrm * (-x * qp), dy = nrm * (-y * qp), dz = nrm * qz;
+            const float zr = ze[l] * R;
+            ex += x * zr + xi[l] * dx;
+            ey += y * zr + xi[l] * dy;
+            ez += z * zr + xi[l] * dz;
+          } else {
+            const float fm = (float)m;
+            const float Cm = eh.C[m], Sm = eh.Sn[m], Cp = eh.C[m - 1], Sp = eh.Sn[m - 1];
+            {  // +m
+              const float R = nrm * q * Cm;
+              const float dx = nrm * (-x * qp * Cm + q * fm * Cp), dy = nrm * (-y * qp * Cm - q * fm * Sp);
+              const float dz = nrm * qz * Cm;
+              const float zr = ze[l + m] * R;
+              ex += x * zr + xi[l + m] * dx;
+              ey += y * zr + xi[l + m] * dy;
+              ez += z * zr + xi[l + m] * dz;
             }
-          }
-          // solid harmonics R_l^m and gradients (index l + m within the l block)
-#pragma unroll
-          for (int m = 0; m <= l; ++m) {
-            const float nrm = c_shnorm[l * (kMaxL + 1) + m];
-            const float q = eh.Q[tri(l, m)];
-            const float qp = (l >= 1 && m + 1 <= l - 1) ? eh.Q[tri(l - 1, m + 1)] : 0.0f;
-            const float qz = (l >= 1 && m <= l - 1) ? (float)(l + m) * eh.Q[tri(l - 1, m)] : 0.0f;
-            if (m == 0) {
-              const float R = nrm * q, dx = nrm * (-x * qp), dy = nrm * (-y * qp), dz = nrm * qz;
-              const float zr = ze[l] * R;
-              ex += x * zr + xi[l] * dx;
-              ey += y * zr + xi[l] * dy;
-              ez += z * zr + xi[l] * dz;
-            } else {
-              const float fm = (float)m;
-              const float Cm = eh.C[m], Sm = eh.Sn[m], Cp = eh.C[m - 1], Sp = eh.Sn[m - 1];
-              {  // +m
-                const float R = nrm * q * Cm;
-                const float dx = nrm * (-x * qp * Cm + q * fm * Cp), dy = nrm * (-y * qp * Cm - q * fm * Sp);
-                const float dz = nrm * qz * Cm;
-                const float zr = ze[l + m] * R;
-                ex += x * zr + xi[l + m] * dx;
-                ey += y * zr + xi[l + m] * dy;
-                ez += z * zr + xi[l + m] * dz;
-              }
-              {  // -m
-                const float R = nrm * q * Sm;
-                const float dx = nrm * (-x * qp * Sm + q * fm * Sp), dy = nrm * (-y * qp * Sm + q * fm * Cp);
-                const float dz = nrm * qz * Sm;
-                const float zr = ze[l - m] * R;
-                ex += x * zr + xi[l - m] * dx;
-                ey += y * zr + xi[l - m] * dy;
-                ez += z * zr + xi[l - m] * dz;
-              }
+            {  // -m
+              const float R = nrm * q * Sm;
+              const float dx = nrm * (-x * qp * Sm + q * fm * Sp), dy = nrm * (-y * qp * Sm + q * fm * Cp);
+              const float dz = nrm * qz * Sm;
+              const float zr = ze[l - m] * R;
+              ex += x * zr + xi[l - m] * dx;
+              ey += y * zr + xi[l - m] * dy;
+              ez += z * zr + xi[l - m] * dz;
             }
           }
         }
-        if (!(a.attach && atom == catom)) {
-          atomicAdd(&a.forces[3 * (size_t)atom + 0], -ex);
-          atomicAdd(&a.forces[3 * (size_t)atom + 1], -ey);
-          atomicAdd(&a.forces[3 * (size_t)atom + 2], -ez);
-          fcx += ex;
-          fcy += ey;
-          fcz += ez;
-        }
       }
-      __syncwarp();
+      if (!(a.attach && atom == catom)) {
+        atomicAdd(&a.forces[3 * (size_t)atom + 0], -ex);
+        atomicAdd(&a.forces[3 * (size_t)atom + 1], -ey);
+        atomicAdd(&a.forces[3 * (size_t)atom + 2], -ez);
+        fcx += ex;
+        fcy += ey;
+        fcz += ez;
+      }
     }
     if (catom >= 0) {
 #pragma unroll
@@ -254,32 +234,48 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
   }
 }
 
+static int resident_blocks(const void* kern, int threads, int smem, int* out) {
+  int occ = 0;
+  int rc = check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem), "occupancy");
+  *out = occ < 1 ? 1 : occ;
+  return rc;
+}
+
 template <int L>
 struct ForceDispatch {
   static int run(const ForceArgs& a, cudaStream_t st) {
-    auto kern = k_forces<L>;
-    const int per_warp = 4 * ForceShape<L>::warp_floats(a.S, a.N);
-    int dev = 0, nsm = 148, smem_sm = 228 * 1024, smem_blk = 227 * 1024;
+    int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    cudaDeviceGetAttribute(&smem_blk, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    // warps per block: the most resident warps per SM (1 KB reserved per block), larger blocks on ties
-    int wpb = 0, best = 0;
-    for (int w = 4; w >= 1; w >>= 1) {
-      const int bytes = w * per_warp;
-      if (bytes > smem_blk) continue;
-      const int resident = w * (smem_sm / (bytes + 1024));
-      if (resident > best) { best = resident; wpb = w; }
+    // G = dE/dc
+    {
+      const int cbytes = 4 * ((a.S * a.N * ((L + 1) * (L + 1) | 1) + 3) & ~3);
+      const bool stage = cbytes + 4 * (int64_t)a.F <= 100 * 1024;
+      auto kern = stage ? k_adjoint_g<L, true> : k_adjoint_g<L, false>;
+      const int smem = cbytes + (stage ? 4 * a.F : 0);
+      int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                          "adjoint smem attribute");
+      if (rc) return rc;
+      int occ = 1;
+      if ((rc = resident_blocks((const void*)kern, kGThreads, smem, &occ))) return rc;
+      int64_t blocks = (int64_t)nsm * occ;
+      if (blocks > a.n_centres) blocks = a.n_centres;
+      kern<<<(unsigned)blocks, kGThreads, smem, st>>>(a);
+      if ((rc = check_launch("k_adjoint_g"))) return rc;
     }
-    if (wpb == 0) return set_error(SOAPB_ERR_UNSUPPORTED, "forces shared memory %d B per warp too large", per_warp);
+    // edges
+    auto kern = k_forces<L>;
+    const int per_warp = 4 * ForceShape<L>::warp_floats(a.S, a.N);
+    int wpb = 4;
+    while (wpb > 1 && wpb * per_warp > 200 * 1024) wpb >>= 1;
+    if (wpb * per_warp > 200 * 1024)
+      return set_error(SOAPB_ERR_UNSUPPORTED, "forces: %d B of shared memory per warp is too large", per_warp);
     const int smem = wpb * per_warp;
     int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                         "forces smem attribute");
     if (rc) return rc;
     int occ = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 * wpb, smem);
-    if (occ < 1) occ = 1;
+    if ((rc = resident_blocks((const void*)kern, 32 * wpb, smem, &occ))) return rc;
     int64_t blocks = (int64_t)nsm * occ;
     const int64_t need = (a.n_centres + wpb - 1) / wpb;
     if (blocks > need) blocks = need;
@@ -293,15 +289,29 @@ struct ForceDispatch {
 
 using namespace soapb;
 
+static int64_t forces_work_bytes(const soapb_basis* b, int64_t n_centres) {
+  const int64_t K = (int64_t)(b->l_max + 1) * (b->l_max + 1);
+  return align_up(4 * n_centres * b->n_species * b->n_max * K, 256);
+}
+
+extern "C" int soapb_forces_workspace(const soapb_basis* b, int64_t n_centres, int64_t* bytes) {
+  if (!b || b->bytes <= 0) return set_error(SOAPB_ERR_ARG, "basis not planned");
+  if (n_centres < 0 || !bytes) return set_error(SOAPB_ERR_ARG, "bad n_centres or null bytes");
+  *bytes = forces_work_bytes(b, n_centres);
+  return SOAPB_OK;
+}
+
 extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
                             const float* d_coeff, const float* d_dEdp, const int32_t* d_centre_atom, int32_t attach,
-                            float* d_forces, int32_t* d_counter, void* stream) {
+                            float* d_forces, void* d_work, int64_t work_bytes, int32_t* d_counter, void* stream) {
   if (!b || !b->dev) return set_error(SOAPB_ERR_ARG, "basis not built");
   if (n_centres < 0 || n_centres >= (int64_t)1 << 31) return set_error(SOAPB_ERR_ARG, "bad n_centres");
   if (n_centres == 0) return SOAPB_OK;
   if (!d_pair_off || !d_coeff || !d_dEdp || !d_forces || !d_counter) return set_error(SOAPB_ERR_ARG, "null argument");
   if (attach && !d_centre_atom) return set_error(SOAPB_ERR_ARG, "attach needs centre atoms");
-  const int N = b->n_max, L = b->l_max;
+  if (!d_work || work_bytes < forces_work_bytes(b, n_centres))
+    return set_error(SOAPB_ERR_ARG, "forces workspace too small (%lld < %lld)", (long long)work_bytes,
+                     (long long)forces_work_bytes(b, n_centres));
   cudaStream_t st = (cudaStream_t)stream;
   ForceArgs a;
   a.pair_off = d_pair_off;
@@ -309,13 +319,14 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.coeff = d_coeff;
   a.dEdp = d_dEdp;
   a.centre_atom = d_centre_atom;
-  a.tab_b = (const float*)((const char*)b->dev + b->off_tab_b);
-  a.tab_bh = (const float*)((const char*)b->dev + b->off_tab_bh);
+  a.tabt_b = (const float*)((const char*)b->dev + b->off_tabt_b);
+  a.tabt_bh = (const float*)((const char*)b->dev + b->off_tabt_bh);
   a.widx = (const int*)((const char*)b->dev + b->off_widx);
+  a.G = (float*)d_work;
   a.forces = d_forces;
   a.counter = d_counter;
   a.n_centres = n_centres;
-  a.N = N;
+  a.N = b->n_max;
   a.S = b->n_species;
   a.nseg = b->n_seg;
   a.F = b->n_feat_ps;
@@ -323,5 +334,5 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.inv_h = (float)(1.0 / b->seg_width);
   int rc = check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st), "reset work counter");
   if (rc) return rc;
-  return dispatch_l<ForceDispatch>(L, a, st);
+  return dispatch_l<ForceDispatch>(b->l_max, a, st);
 }

@@ -399,9 +399,12 @@ class SOAP:
     def _run_forces(self, batch, pairs, coeff, dEdp, attach=True):
         lib = _lib.load()
         forces = torch.zeros((batch.n_atoms, 3), dtype=torch.float32, device=self.device)
+        wsb = ctypes.c_int64(0)
+        check(lib.soapb_forces_workspace(ctypes.byref(self._basis), batch.n_centres, ctypes.byref(wsb)))
+        work = torch.empty(max(int(wsb.value), 256), dtype=torch.uint8, device=self.device)
         self._call("forces", lib.soapb_forces, ctypes.byref(self._basis), batch.n_centres, _ptr(pairs.pair_off),
                    _ptr(pairs.pairs), _ptr(coeff), _ptr(dEdp), _ptr(batch.centre_attach), int(bool(attach)),
-                   _ptr(forces), _ptr(self._counter), _stream(self.device))
+                   _ptr(forces), _ptr(work), work.numel(), _ptr(self._counter), _stream(self.device))
         return forces
 
     def _out_mode(self) -> int:

@@ -68,6 +68,7 @@ typedef struct soapb_basis {
   int32_t n_feat_cc; /* SG:909-910 */
   int64_t bytes;     /* device bytes the basis needs */
   int64_t off_alpha, off_beta, off_tab_b, off_tab_bh, off_ftab, off_widx, off_err;  /* byte offsets into dev */
+  int64_t off_tabt_b, off_tabt_bh; /* function-major copies of the radial tables */
   void* dev;         /* set by soapb_basis_build */
 } soapb_basis;
 
@@ -194,11 +195,13 @@ int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int64_t* d_pai
  * d_forces[a] += -dE/dx_a (float32 (n_atoms, 3); the caller zeroes it) with
  * float atomics.  attach = 1: centres move with their atoms (d_centre_atom);
  * 0: fixed centres.  d_coeff: raw coefficients on SOAPB_NL_ALL pairs.
- * d_counter: one int32 of scratch.  Replaces one reverse pass of the
- * reference's autograd Jacobian SG:2007-2113 without materialising dp/dr. */
+ * d_work: soapb_forces_workspace bytes (G = dE/dc per centre).  d_counter:
+ * one int32 of scratch.  Replaces one reverse pass of the reference's
+ * autograd Jacobian SG:2007-2113 without materialising dp/dr. */
+int soapb_forces_workspace(const soapb_basis* b, int64_t n_centres, int64_t* bytes);
 int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
                  const float* d_coeff, const float* d_dEdp, const int32_t* d_centre_atom, int32_t attach,
-                 float* d_forces, int32_t* d_counter, void* stream);
+                 float* d_forces, void* d_work, int64_t work_bytes, int32_t* d_counter, void* stream);
 
 /* Message describing the last error on the calling thread ("" if none). */
 const char* soapb_last_error(void);
