@@ -9,14 +9,17 @@
 // in the reference (coeffs_use = coeffs, :1651-1657), i.e. identical to 'off'.
 //
 // Mapping: one warp per centre, centres taken from an atomic work queue.
-// Each lane owns one radial function (n, l) ("single": N (L+1) <= 32) or two
-// with l0 + l1 = L ("paired"), and keeps their 2l+1 m-accumulators in
-// registers.  The centre's pairs arrive sorted by (species, radial segment):
-// the species switch flushes the accumulators into the warp's coefficient
-// buffer, the segment switch (warp-uniform) reloads the lane's table
-// coefficients, so the per-pair work is 7 FMAs of Horner per function plus
-// one FMA per (n, l, m).  Solid harmonics are computed 32 pairs at a time,
-// one pair per lane, into shared memory.
+// Lanes are grouped by l: floor(32 / (L+1)) lanes per l, each owning GN radial
+// functions (n, l) of the same l, so one shared-memory read of R_lm feeds GN
+// accumulators and the m loop is the same for all of them.  The centre's
+// pairs arrive sorted by (species, radial segment): the species switch
+// flushes the accumulators into the warp's coefficient buffer, the segment
+// switch (warp-uniform) reloads the lane's table coefficients, so the
+// per-pair work is 7 FMAs of Horner per function plus one FMA per (n, l, m).
+// Solid harmonics are computed 32 pairs at a time, one pair per lane, into
+// shared memory.  The power-spectrum epilogue walks the DScribe blocks
+// (species pair, l) with the m loop unrolled per l; each lane writes
+// consecutive features, so the row is stored coalesced.
 #include "common.cuh"
 
 namespace soapb {
@@ -26,11 +29,10 @@ struct DescArgs {
   const float4* pairs;
   int64_t n_centres;
   const float* tab_b;
-  const int* ftab;
   float* out;
   float* coeff_out;  // optional raw c[s][n][lm] rows (S N K floats per centre)
   int* counter;
-  int N, S, nseg, F, mode;
+  int N, S, nseg, F, mode, crossover;
   float inv_h;
 };
 
@@ -42,13 +44,18 @@ struct DescShape {
   __host__ __device__ static int warp_floats(int S, int N) { return 32 * YS + 96 + S * N * KC; }
 };
 
-template <int L, bool PAIRED>
+constexpr int kMaxBlocks = kMaxS * (kMaxS + 1) / 2;
+constexpr int kMaxTri = kMaxN * (kMaxN + 1) / 2;
+
+template <int L, int GN>
 __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
   using Sh = DescShape<L>;
-  constexpr int K = Sh::K, YS = Sh::YS, KC = Sh::KC;
-  constexpr int MT = PAIRED ? 2 * L + 2 : 2 * L + 1;
+  constexpr int K = Sh::K, YS = Sh::YS, KC = Sh::KC, M = 2 * L + 1;
+  constexpr int LPL = 32 / (L + 1);  // lanes per l
   extern __shared__ float sm[];
   __shared__ float s_pref[kMaxL + 1];
+  __shared__ int s_blk[2 * kMaxBlocks];              // (j | jd << 8, first feature) per species block
+  __shared__ unsigned char s_tri[2 * kMaxTri];       // (n, n') of the upper-triangle index
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int N = a.N, S = a.S, NF = N * (L + 1);
   const int cbn = S * N * KC;
@@ -58,15 +65,30 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
   int* spp = sg + 32;
   float* cbuf = (float*)(spp + 32);
   if (threadIdx.x <= L) s_pref[threadIdx.x] = sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * threadIdx.x + 1.0f));
+  if (threadIdx.x == 0) {
+    int nb = 0, f = 0;
+    for (int j = 0; j < S; ++j)
+      for (int jd = j; jd < (a.crossover ? S : j + 1); ++jd) {
+        s_blk[2 * nb] = j | (jd << 8);
+        s_blk[2 * nb + 1] = f;
+        f += (j == jd ? N * (N + 1) / 2 : N * N) * (L + 1);
+        ++nb;
+      }
+    int p = 0;
+    for (int n = 0; n < N; ++n)
+      for (int nd = n; nd < N; ++nd, ++p) {
+        s_tri[2 * p] = (unsigned char)n;
+        s_tri[2 * p + 1] = (unsigned char)nd;
+      }
+  }
   __syncthreads();
+  const int nblk = a.crossover ? S * (S + 1) / 2 : S;
 
-  const LaneFns lf = lane_fns(lane, N, L, PAIRED);
-  const int m0 = lf.l0 >= 0 ? 2 * lf.l0 + 1 : 0;
-  const int mtot = m0 + (lf.l1 >= 0 ? 2 * lf.l1 + 1 : 0);
-  const int yoff0 = lf.l0 >= 0 ? lf.l0 * lf.l0 : 0;
-  const int yoff1 = lf.l1 >= 0 ? lf.l1 * lf.l1 - m0 : 0;
-  const int fn0 = lf.l0 >= 0 ? fn_index(lf.n0, lf.l0, N) : 0;
-  const int fn1 = lf.l1 >= 0 ? fn_index(lf.n1, lf.l1, N) : 0;
+  // lane -> l and its functions n = k GN + g
+  const int l_me = lane / LPL, k_me = lane % LPL;
+  const bool active = l_me <= L && k_me * GN < N;
+  const int lme = active ? l_me : 0;
+  const int mme = 2 * lme + 1;
 
   for (;;) {
     int c32 = 0;
@@ -74,26 +96,37 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
     const int64_t c = __shfl_sync(0xffffffffu, c32, 0);
     if (c >= a.n_centres) break;
     for (int i = lane; i < cbn; i += 32) cbuf[i] = 0.0f;
-    float acc[MT];
+    float acc[GN][M];
 #pragma unroll
-    for (int k = 0; k < MT; ++k) acc[k] = 0.0f;
-    float cf0[kNCoef], cf1[kNCoef];
+    for (int g = 0; g < GN; ++g)
 #pragma unroll
-    for (int k = 0; k < kNCoef; ++k) { cf0[k] = 0.0f; cf1[k] = 0.0f; }
+      for (int m = 0; m < M; ++m) acc[g][m] = 0.0f;
+    float cf[GN][kNCoef];
+#pragma unroll
+    for (int g = 0; g < GN; ++g)
+#pragma unroll
+      for (int k = 0; k < kNCoef; ++k) cf[g][k] = 0.0f;
     int cur_sp = -1, cur_seg = -1;
     const int64_t p0 = a.pair_off[c], p1 = a.pair_off[c + 1];
     __syncwarp();
 
     auto flush = [&](int sp) {
+      if (active) {
 #pragma unroll
-      for (int k = 0; k < MT; ++k) {
-        if (k < mtot) {
-          const bool first = k < m0;
-          const int n = first ? lf.n0 : lf.n1, l = first ? lf.l0 : lf.l1, m = first ? k : k - m0;
-          cbuf[(sp * N + n) * KC + l * l + m] += acc[k];
+        for (int g = 0; g < GN; ++g) {
+          const int n = k_me * GN + g;
+          if (n < N) {
+            float* dst = cbuf + (sp * N + n) * KC + lme * lme;
+#pragma unroll
+            for (int m = 0; m < M; ++m)
+              if (m < mme) dst[m] += acc[g][m];
+          }
         }
-        acc[k] = 0.0f;
       }
+#pragma unroll
+      for (int g = 0; g < GN; ++g)
+#pragma unroll
+        for (int m = 0; m < M; ++m) acc[g][m] = 0.0f;
     };
 
     for (int64_t base = p0; base < p1; base += 32) {
@@ -120,19 +153,26 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
         }
         const int seg = sg[q];
         if (seg != cur_seg) {
-          if (lf.l0 >= 0) load_coef(a.tab_b, seg, fn0, NF, cf0);
-          if (PAIRED && lf.l1 >= 0) load_coef(a.tab_b, seg, fn1, NF, cf1);
+          if (active) {
+#pragma unroll
+            for (int g = 0; g < GN; ++g) {
+              const int n = k_me * GN + g;
+              if (n < N) load_coef(a.tab_b, seg, fn_index(n, lme, N), NF, cf[g]);
+            }
+          }
           cur_seg = seg;
         }
         const float t = tt[q];
-        const float B0 = horner7(cf0, t);
-        const float B1 = PAIRED ? horner7(cf1, t) : 0.0f;
-        const float* yr = Y + q * YS;
+        float B[GN];
 #pragma unroll
-        for (int k = 0; k < MT; ++k) {
-          if (k < mtot) {
-            const bool first = k < m0;
-            acc[k] = fmaf(first ? B0 : B1, yr[k + (first ? yoff0 : yoff1)], acc[k]);
+        for (int g = 0; g < GN; ++g) B[g] = horner7(cf[g], t);
+        const float* yr = Y + q * YS + lme * lme;
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          if (m < mme) {
+            const float yv = yr[m];
+#pragma unroll
+            for (int g = 0; g < GN; ++g) acc[g][m] = fmaf(B[g], yv, acc[g][m]);
           }
         }
       }
@@ -150,17 +190,31 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
     }
     float* orow = a.out + (size_t)c * a.F;
     if (a.mode == SOAPB_OUT_PS) {
-      for (int f = lane; f < a.F; f += 32) {
-        const int code = __ldg(a.ftab + f);
-        const int j = code & 15, jd = (code >> 4) & 15, n = (code >> 8) & 31, nd = (code >> 13) & 31,
-                  l = (code >> 18) & 31;
-        const float* x = cbuf + (j * N + n) * KC + l * l;
-        const float* y = cbuf + (jd * N + nd) * KC + l * l;
-        float s = 0.0f;
+      for (int b = 0; b < nblk; ++b) {
+        const int jj = s_blk[2 * b], fb0 = s_blk[2 * b + 1];
+        const int j = jj & 255, jd = jj >> 8;
+        const bool diag = j == jd;
+        const int np = diag ? N * (N + 1) / 2 : N * N;
 #pragma unroll
-        for (int m = 0; m < 2 * L + 1; ++m)
-          if (m < 2 * l + 1) s = fmaf(x[m], y[m], s);
-        orow[f] = s * s_pref[l];
+        for (int l = 0; l <= L; ++l) {
+          float* o = orow + fb0 + l * np;
+          for (int p = lane; p < np; p += 32) {
+            int n, nd;
+            if (diag) {
+              n = s_tri[2 * p];
+              nd = s_tri[2 * p + 1];
+            } else {
+              n = p / N;
+              nd = p - n * N;
+            }
+            const float* x = cbuf + (j * N + n) * KC + l * l;
+            const float* y = cbuf + (jd * N + nd) * KC + l * l;
+            float s = 0.0f;
+#pragma unroll
+            for (int m = 0; m < 2 * l + 1; ++m) s = fmaf(x[m], y[m], s);
+            o[p] = s * s_pref[l];
+          }
+        }
       }
     } else {
       const bool cc = a.mode == SOAPB_OUT_CC;
@@ -181,14 +235,22 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
   }
 }
 
-template <int L, bool PAIRED>
+// Functions per lane for (N, L): floor(32 / (L+1)) lanes share each l.
+inline int desc_group(int N, int L) {
+  const int lpl = 32 / (L + 1);
+  int gn = (N + lpl - 1) / lpl;
+  if (gn == 5) gn = 6;
+  return gn;
+}
+
+template <int L, int GN>
 static int launch_descriptor(const DescArgs& a, cudaStream_t st) {
   const int per_warp = 4 * DescShape<L>::warp_floats(a.S, a.N);
   int wpb = (200 * 1024) / per_warp;
   wpb = wpb > 4 ? 4 : wpb;
   if (wpb < 1) return set_error(SOAPB_ERR_UNSUPPORTED, "descriptor shared memory %d B per warp too large", per_warp);
   const int smem = wpb * per_warp;
-  auto kern = k_descriptor<L, PAIRED>;
+  auto kern = k_descriptor<L, GN>;
   int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                       "descriptor smem attribute");
   if (rc) return rc;
@@ -207,8 +269,15 @@ static int launch_descriptor(const DescArgs& a, cudaStream_t st) {
 
 template <int L>
 struct DescDispatch {
-  static int run(const DescArgs& a, bool paired, cudaStream_t st) {
-    return paired ? launch_descriptor<L, true>(a, st) : launch_descriptor<L, false>(a, st);
+  static int run(const DescArgs& a, int gn, cudaStream_t st) {
+    switch (gn) {
+      case 1: return launch_descriptor<L, 1>(a, st);
+      case 2: return launch_descriptor<L, 2>(a, st);
+      case 3: return launch_descriptor<L, 3>(a, st);
+      case 4: return launch_descriptor<L, 4>(a, st);
+      case 6: return launch_descriptor<L, 6>(a, st);
+      default: return set_error(SOAPB_ERR_UNSUPPORTED, "descriptor: %d radial functions per lane not built", gn);
+    }
   }
 };
 
@@ -226,17 +295,12 @@ extern "C" int soapb_descriptor(const soapb_basis* b, int64_t n_centres, const i
   if (n_centres == 0) return SOAPB_OK;
   if (!d_pair_off || !d_out || !d_counter) return set_error(SOAPB_ERR_ARG, "null argument");
   const int N = b->n_max, L = b->l_max;
-  bool paired;
-  if (N * (L + 1) <= 32) paired = false;
-  else if (lanes_needed(N, L, true) <= 32) paired = true;
-  else return set_error(SOAPB_ERR_UNSUPPORTED, "n_max * (l_max + 1) = %d radial functions exceed one warp", N * (L + 1));
   cudaStream_t st = (cudaStream_t)stream;
   DescArgs a;
   a.pair_off = d_pair_off;
   a.pairs = (const float4*)d_pairs;
   a.n_centres = n_centres;
   a.tab_b = (const float*)((const char*)b->dev + b->off_tab_b);
-  a.ftab = (const int*)((const char*)b->dev + b->off_ftab);
   a.out = d_out;
   a.coeff_out = d_coeff;
   a.counter = d_counter;
@@ -245,8 +309,9 @@ extern "C" int soapb_descriptor(const soapb_basis* b, int64_t n_centres, const i
   a.nseg = b->n_seg;
   a.F = out_mode == SOAPB_OUT_PS ? b->n_feat_ps : b->n_feat_cc;
   a.mode = out_mode;
+  a.crossover = b->crossover ? 1 : 0;
   a.inv_h = (float)(1.0 / b->seg_width);
   int rc = check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st), "reset work counter");
   if (rc) return rc;
-  return dispatch_l<DescDispatch>(L, a, paired, st);
+  return dispatch_l<DescDispatch>(L, a, desc_group(N, L), st);
 }
