@@ -219,8 +219,8 @@ def batched_vs_plain(soap_cls, torch):
             d = dict(c)
             d["positions"] = c["positions"].clone().requires_grad_(True)
             sysl.append(d)
-        out = soap.create(sysl)
-        E = sum((o * w).sum() for o in out) if isinstance(out, list) else (out * w).sum()
+        out = soap.create(sysl)  # a list: the cells differ in size
+        E = ((torch.cat(out) if isinstance(out, list) else out) * w).sum()
         E.backward()
         return sysl
 
@@ -266,7 +266,7 @@ def run_batched_only(args):
     def one():
         sysl = [dict(c, positions=c["positions"].clone().requires_grad_(True)) for c in dev_cells]
         out = soap.create(sysl)
-        E = sum((o * w).sum() for o in out) if isinstance(out, list) else (out * w).sum()
+        E = ((torch.cat(out) if isinstance(out, list) else out) * w).sum()
         E.backward()
 
     one()
@@ -282,6 +282,55 @@ def run_batched_only(args):
     n_atoms = sum(len(c["atomic_numbers"]) for c in cells)
     print(json.dumps({"workload": f"first {len(cells)} cells of the 512-cell batch ({n_atoms} atoms)",
                       "ms_per_step": e0.elapsed_time(e1) / args.steps, "stage_ms_per_step": st}), flush=True)
+
+
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA at the 1965 MHz max clock
+
+
+def scale_create(soap_cls, torch, steps: int = 3, warmup: int = 2):
+    """The scale workload: create() on the 1,000,002-atom water cluster
+    (n_max 8, l_max 4, F = 680, 2.72 GB of output), positions resident on the
+    device.  Reports atoms/s and the descriptor kernel against both its HBM
+    traffic (pairs read + rows written) and its FP32 work."""
+    from cusoap_b200 import workloads as W
+    sysd = W.make("cluster1M")
+    soap = soap_cls(**W.CONFIGS["cluster1M"])
+    pos = torch.tensor(sysd["positions"], dtype=torch.float64, device="cuda")
+    system = {"positions": pos, "atomic_numbers": sysd["atomic_numbers"]}
+    for _ in range(warmup):
+        out = soap.create(system)
+        del out
+    torch.cuda.synchronize()
+    soap.profile = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        out = soap.create(system)
+        del out
+    e1.record()
+    torch.cuda.synchronize()
+    st = {k: v / steps for k, v in soap.stage_times().items()}
+    soap.profile = None
+    n_at, F = len(sysd["atomic_numbers"]), soap.get_number_of_features()
+    # pairs: the last create's list length (same every step)
+    from cusoap_b200.soap import _Batch, _Pairs
+    from cusoap_b200 import _lib
+    n_pairs = _Pairs(soap, _Batch(soap, [system], [None]), _lib.NL_CREATE).total
+    N, L = W.CONFIGS["cluster1M"]["n_max"], W.CONFIGS["cluster1M"]["l_max"]
+    K = (L + 1) ** 2
+    flop = n_pairs * (2 * N * K + N * (L + 1) * 16) + n_at * 2 * F * K / (L + 1)
+    byts = n_pairs * 16 + n_at * F * 4
+    d_ms = st.get("descriptor", float("nan"))
+    peak, _ = _peaks()
+    return {"workload": "(H2O)_333334 non-periodic cluster, 1,000,002 atoms; r_cut 6, n_max 8, l_max 4, sigma 1; "
+                        "create() only, positions on the device",
+            "atoms_per_s": n_at * steps / (e0.elapsed_time(e1) / 1e3), "ms_per_step": e0.elapsed_time(e1) / steps,
+            "stage_ms_per_step": st, "pairs": n_pairs,
+            "descriptor": {"hbm_bytes": byts, "gbs": byts / d_ms / 1e6, "hbm_frac_of_measured": byts / d_ms / 1e6 / peak,
+                           "flop": flop, "tflops": flop / d_ms / 1e9,
+                           "fp32_frac_of_nominal": flop / d_ms / 1e9 / FP32_PEAK_TFLOPS,
+                           "note": "flop = pairs x (2 N K accumulate + 16 N (l_max+1) radial Horner) + centres x "
+                                   "2 F K/(l_max+1) power spectrum; bytes = 16 B per pair read + F x 4 B per row"}}
 
 
 def run_ours(args):
@@ -395,6 +444,13 @@ def run_ours(args):
         except Exception as exc:  # reported, never silently dropped
             extra = {"error": repr(exc)}
 
+    scale = None
+    if not args.no_batched and rank == 0 and args.nx == 10:
+        try:
+            scale = scale_create(SOAP, torch)
+        except Exception as exc:  # reported, never silently dropped
+            scale = {"error": repr(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and args.nx == 10:
         cpu = cpu_baseline_sample()
@@ -410,7 +466,7 @@ def run_ours(args):
             "config": dict(CONFIG, parallelism=f"replicas x{world}" if world > 1 else "single GPU")
             if args.nx == 10 else {"workload": f"profiling case: {n_at}-atom water cluster, same parameters"},
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk, "cpu_baseline": cpu,
-            "batched_vs_plain": extra}
+            "batched_vs_plain": extra, "scale_create": scale}
     print(json.dumps(line), flush=True)
 
 
@@ -428,8 +484,15 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batched-cells", type=int, default=0,
                     help="profiling case: run only the batched path on the first K cells")
+    ap.add_argument("--scale-only", action="store_true",
+                    help="profiling case: run only the 1,000,002-atom create() leg and print its object")
     args = ap.parse_args()
-    if args.batched_cells > 0:
+    if args.scale_only:
+        import torch
+        from cusoap_b200 import SOAP
+        torch.cuda.set_device(0)
+        print(json.dumps(scale_create(SOAP, torch, steps=args.steps, warmup=args.warmup)), flush=True)
+    elif args.batched_cells > 0:
         run_batched_only(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -9,6 +9,9 @@ It restates, in vectorised numpy float64, the algorithm of the reference
 ``src/cusoap/soap_generator.py`` (cited below as ``SG:<line>``):
 
 * GTO basis and Loewdin S^-1/2 ........................ SG:690-708, SG:339-343
+* polynomial basis (sqrtm(inv(S)), Gauss-Legendre grid)  SG:350-362, SG:710-752
+* polynomial radial integrals (scaled Bessel recurrence)  SG:477-508, SG:1432-1594
+* weighting functions (poly / pow / exp, w0, r_cut) .... SG:403-470, SG:584-597
 * periodic images (perpendicular widths, offsets) ...... SG:369-396, SG:1015-1021
 * radius neighbour list, r~0 edge drop ................. SG:1042-1181
 * GTO coefficients c_nlm (primitive radial x Y, beta) .. SG:1294-1391
@@ -84,6 +87,152 @@ def radial_B_Bhat(r2: np.ndarray, betas, gamma, pref):
     B = np.einsum("elk,lnk->enl", Q, betas)
     Bhat = np.einsum("elk,lnk->enl", (-2.0 * gamma[None]) * Q, betas)
     return B, Bhat
+
+
+def gauss_legendre(n: int) -> Tuple[np.ndarray, np.ndarray]:
+    """Nodes and weights on [-1, 1] by the Golub-Welsch eigenproblem (SG:350-362)."""
+    k = np.arange(1, n, dtype=np.float64)
+    beta = k / np.sqrt(4.0 * k * k - 1.0)
+    J = np.diag(beta, 1) + np.diag(beta, -1)
+    x, V = np.linalg.eigh(J)
+    return x, 2.0 * V[0, :] ** 2
+
+
+def poly_basis(r_cut: float, n_max: int, quad_n: int = 100):
+    """DScribe polynomial basis g_n(r) = sum_k beta_nk (r_cut - r)^(k+2) on the
+    Gauss-Legendre grid: (rx, wr, gss (n_max, Q)), beta = sqrtm(inv(S)) in
+    float64 exactly as the reference computes it (SG:710-752)."""
+    from scipy.linalg import sqrtm
+    n, rc = int(n_max), float(r_cut)
+    S = np.zeros((n, n))
+    for i in range(1, n + 1):
+        for j in range(1, n + 1):
+            S[i - 1, j - 1] = (2 * rc ** (7 + i + j)) / ((5 + i + j) * (6 + i + j) * (7 + i + j))
+    betas = sqrtm(np.linalg.inv(S))
+    if np.iscomplexobj(betas):
+        raise ValueError("Could not calculate normalization factors for the radial basis in the domain of real "
+                         "numbers. Lowering the number of radial basis functions (n_max) or increasing the radial "
+                         "cutoff (r_cut) is advised.")
+    x, w = gauss_legendre(quad_n)
+    rx = rc * 0.5 * (x + 1.0)
+    wr = rc * 0.5 * w
+    rclip = np.clip(rx, 0.0, rc)
+    fs = np.stack([(rc - rclip) ** (k + 2) for k in range(1, n + 1)])
+    return rx, wr, np.ascontiguousarray(betas) @ fs
+
+
+def poly_I_J(r, rx, wr, gss, eta, l_max, want_J):
+    """I[e,n,l] = 4 pi int rx^2 g_n e^{-eta (rx-r)^2} ie_l(t) drx and
+    J[e,n,l] = 4 pi int rx^3 g_n e^{-eta (rx-r)^2} ie_{l+1}(t) drx, t = 2 eta rx r,
+    ie_l = i_l e^{-t} by the upward recurrence with the reference's clamps
+    (SG:477-508, SG:1432-1510)."""
+    r = np.asarray(r, np.float64)
+    Lp1 = l_max + 1
+    tt = np.clip(2.0 * eta * rx[None, :] * r[:, None], 1e-12, None)
+    e2 = np.exp(-2.0 * tt)
+    oOt = 1.0 / tt
+    common = 4.0 * math.pi * (rx * rx * wr)[None, :] * np.exp(-eta * (rx[None, :] - r[:, None]) ** 2)
+    I = np.empty((len(r), gss.shape[0], Lp1))
+    J = np.empty_like(I) if want_J else None
+    L_top = Lp1 if want_J else Lp1 - 1
+    P_pp = P_p = None
+    for l in range(L_top + 1):
+        if l == 0:
+            P = common * ((1.0 - e2) * (0.5 * oOt))
+        elif l == 1:
+            P = common * np.clip((1.0 + e2) * (0.5 * oOt) - (1.0 - e2) * (0.5 * oOt * oOt), 0.0, None)
+        else:
+            P = np.minimum(np.clip(P_pp - (2 * l - 1) * oOt * P_p, 0.0, None), P_p)
+        if l < Lp1:
+            I[:, :, l] = P @ gss.T
+        if want_J and l >= 1:
+            J[:, :, l - 1] = (P * rx[None, :]) @ gss.T
+        P_pp, P_p = P_p, P
+    return I, J
+
+
+def poly_B_Bhat_r0(rx, wr, gss, eta, l_max):
+    """Exact r -> 0 limits of B_nl = I_nl / r^l and Bhat_nl (SG:1512-1543)."""
+    common0 = 4.0 * math.pi * rx * rx * wr * np.exp(-eta * rx * rx)
+    B0 = np.empty((gss.shape[0], l_max + 1))
+    Bh0 = np.empty_like(B0)
+    fl = np.ones_like(rx)
+    df = 1.0
+    for l in range(l_max + 1):
+        df_next = df * (2 * l + 3)
+        B0[:, l] = (common0 * fl / df) @ gss.T
+        Bh0[:, l] = 2.0 * eta * ((common0 * fl * 2.0 * eta * rx * rx / df_next) @ gss.T - B0[:, l])
+        fl = fl * 2.0 * eta * rx
+        df = df_next
+    return B0, Bh0
+
+
+def poly_B_Bhat(r, rx, wr, gss, eta, l_max):
+    """B = I / r^l, Bhat = 2 eta (J - r I) / r^(l+1); edges with r < 1e-4 take
+    the exact limits (SG:1545-1594)."""
+    r = np.asarray(r, np.float64)
+    tiny = r < 1e-4
+    rs = np.where(tiny, 1.0, r)
+    I, J = poly_I_J(rs, rx, wr, gss, eta, l_max, want_J=True)
+    rl = rs[:, None] ** np.arange(l_max + 1)[None, :]
+    B = I / rl[:, None, :]
+    Bh = 2.0 * eta * (J - rs[:, None, None] * I) / (rl * rs[:, None])[:, None, :]
+    if tiny.any():
+        B0, Bh0 = poly_B_Bhat_r0(rx, wr, gss, eta, l_max)
+        B[tiny] = B0
+        Bh[tiny] = Bh0
+    return B, Bh
+
+
+class Weighting:
+    """DScribe weighting w(r) (SG:403-470) and its radial derivative, which the
+    reference gets from autograd through the same expression."""
+
+    def __init__(self, function=None, r0=1.0, c=1.0, d=1.0, m=1.0, w0=1.0):
+        self.function, self.r0, self.c, self.d, self.m, self.w0 = function, float(r0), float(c), float(d), \
+            float(m), float(w0)
+
+    def infer_rcut(self, threshold=1e-2) -> float:
+        fn = self.function
+        if fn is None:
+            raise ValueError("Cannot infer r_cut when weighting.function is None; provide r_cut explicitly.")
+        if fn == "poly":
+            return self.r0
+        val = self.c / threshold - self.d
+        if val <= 0:
+            raise ValueError(f"Invalid weighting: c/threshold - d must be >0 for {fn}.")
+        if fn == "pow":
+            return self.r0 * val ** (1.0 / self.m)
+        if fn == "exp":
+            return -self.r0 * math.log(val)
+        raise ValueError(f"Unknown weighting function: {fn}")
+
+    def value_and_derivative(self, r):
+        """(w, dw/dr) for r >= 0; w0 (and slope 0) on r < 1e-12."""
+        r = np.asarray(r, np.float64)
+        if self.function is None:
+            w, dw = np.ones_like(r), np.zeros_like(r)
+        elif self.function == "poly":
+            x = r / self.r0
+            base = 1.0 + 2.0 * x ** 3 - 3.0 * x ** 2
+            inside = (r <= self.r0) & (base > 0)
+            bpos = np.where(inside, base, 1.0)
+            w = np.where(inside, self.c * bpos ** self.m, 0.0)
+            dw = np.where(inside, self.c * self.m * bpos ** (self.m - 1.0) * (6.0 * x * x - 6.0 * x) / self.r0, 0.0)
+        elif self.function == "pow":
+            x = r / self.r0
+            xm = x ** self.m
+            w = self.c / (self.d + xm)
+            xm1 = np.where(x > 0, x ** (self.m - 1.0), 0.0 if self.m > 1 else (1.0 if self.m == 1 else np.inf))
+            dw = -self.c * self.m * xm1 / self.r0 / (self.d + xm) ** 2
+        elif self.function == "exp":
+            e = np.exp(-r / self.r0)
+            w = self.c / (self.d + e)
+            dw = self.c * e / self.r0 / (self.d + e) ** 2
+        else:
+            raise ValueError(f"Unknown weighting function: {self.function}")
+        tiny = r < 1e-12
+        return np.where(tiny, self.w0, w), np.where(tiny, 0.0, dw)
 
 
 # ---------------------------------------------------------------------------
@@ -186,11 +335,22 @@ def pbc_offsets(cell: np.ndarray, pbc, cutoff: float) -> np.ndarray:
 # ---------------------------------------------------------------------------
 
 class OracleSOAP:
-    """FP64 oracle with the reference constructor semantics (SG:524-634) for
-    rbf='gto', weighting=None (the configuration every workload here uses)."""
+    """FP64 oracle with the reference constructor semantics (SG:524-634):
+    rbf 'gto' or 'polynomial', optional DScribe weighting."""
 
-    def __init__(self, r_cut, n_max, l_max, sigma=1.0, species=(1,), crossover=True,
-                 average="off", periodic=False):
+    def __init__(self, r_cut=None, n_max=None, l_max=None, sigma=1.0, species=(1,), crossover=True,
+                 average="off", periodic=False, rbf="gto", weighting=None, quad_n=100):
+        self.weighting = None
+        thr = 1e-2
+        if weighting is not None:
+            wd = dict(weighting)
+            thr = float(wd.pop("threshold", 1e-2))
+            self.weighting = Weighting(**wd)
+        if r_cut is None:
+            if self.weighting is None:
+                raise ValueError("Either r_cut or weighting must be provided.")
+            r_cut = self.weighting.infer_rcut(thr)
+        self.rbf = str(rbf).lower()
         self.r_cut = float(r_cut)
         self.n_max = int(n_max)
         self.l_max = int(l_max)
@@ -204,11 +364,40 @@ class OracleSOAP:
         self.periodic = bool(periodic)
         # cutoff padding for the gaussian tails, threshold 1e-3 (SG:600-602)
         self.cutoff = self.r_cut + self.sigma * math.sqrt(-2.0 * math.log(1e-3))
-        self.alphas, self.betas = gto_basis(self.r_cut, self.n_max, self.l_max)
-        self.gamma, self.pref = radial_tables(self.alphas, self.betas, self.eta)
+        if self.rbf == "gto":
+            self.alphas, self.betas = gto_basis(self.r_cut, self.n_max, self.l_max)
+            self.gamma, self.pref = radial_tables(self.alphas, self.betas, self.eta)
+        elif self.rbf == "polynomial":
+            self.rx, self.wr, self.gss = poly_basis(self.r_cut, self.n_max, quad_n)
+        else:
+            raise ValueError("rbf must be 'gto' or 'polynomial'.")
         self.K = (self.l_max + 1) ** 2
         self.l_of_lm = np.array([l for l in range(self.l_max + 1) for _ in range(2 * l + 1)])
         self._build_feature_table()
+
+    # ---- radial factors of one edge: c_nlm = B_nl R_lm, dB/drvec = rvec Bhat ----
+    def radial_unweighted(self, r2):
+        r2 = np.asarray(r2, np.float64)
+        if self.rbf == "gto":
+            return radial_B_Bhat(r2, self.betas, self.gamma, self.pref)
+        return poly_B_Bhat(np.sqrt(r2), self.rx, self.wr, self.gss, self.eta, self.l_max)
+
+    def radial(self, r2):
+        """B[e,n,l], Bhat[e,n,l] including the weighting: w B and
+        w Bhat + (dw/dr / r) B; r < 1e-12 edges take w0 (SG:466-469)."""
+        B, Bh = self.radial_unweighted(r2)
+        if self.weighting is None:
+            return B, Bh
+        r = np.sqrt(np.asarray(r2, np.float64))
+        w, dw = self.weighting.value_and_derivative(r)
+        rs = np.where(r < 1e-12, 1.0, r)
+        return w[:, None, None] * B, w[:, None, None] * Bh + (dw / rs)[:, None, None] * B
+
+    def self_l0(self):
+        """l = 0 value of the centre's own Gaussian, w0 B_n0(0) Y00 (SG:765-797)."""
+        B0, _ = self.radial_unweighted(np.zeros(1))
+        w0 = self.weighting.w0 if self.weighting is not None else 1.0
+        return w0 * B0[0, :, 0] * Y00
 
     # ---- feature bookkeeping (SG:908-962, SG:1215-1245) ----
     def n_power_features(self) -> int:
@@ -334,8 +523,7 @@ class OracleSOAP:
         if not keep_self:
             # analytic self term (SG:765-785, SG:821-850): B_n0(0) * Y00 on the
             # centre's own species, l=0
-            B0, _ = radial_B_Bhat(np.zeros(1), self.betas, self.gamma, self.pref)
-            self_l0 = B0[0, :, 0] * Y00
+            self_l0 = self.self_l0()
             for k in range(C):
                 if cidx[k] >= 0:
                     c[k, self.z2s[int(Z[cidx[k]])], :, 0] += self_l0
@@ -347,7 +535,7 @@ class OracleSOAP:
         for s0 in range(0, len(ci), chunk):
             rvc = rv[s0:s0 + chunk]
             r2 = (rvc * rvc).sum(1)
-            B, _ = radial_B_Bhat(r2, self.betas, self.gamma, self.pref)
+            B, _ = self.radial(r2)
             R = solid_harmonics(rvc, self.l_max)
             contrib = (B[:, :, self.l_of_lm] * R[:, None, :]).reshape(len(rvc), N * K)
             np.add.at(out, ci[s0:s0 + chunk] * S + sp[s0:s0 + chunk], contrib)
@@ -412,7 +600,7 @@ class OracleSOAP:
         N, K, S, Lp1 = self.n_max, self.K, self.S, self.l_max + 1
         F = self.n_features()
         r2 = (rv * rv).sum(1)
-        B, Bh = radial_B_Bhat(r2, self.betas, self.gamma, self.pref)
+        B, Bh = self.radial(r2)
         R, dR = solid_harmonics(rv, self.l_max, gradients=True)
         Bl, Bhl = B[:, :, self.l_of_lm], Bh[:, :, self.l_of_lm]
         cE = (Bl * R[:, None, :])
@@ -471,7 +659,7 @@ class OracleSOAP:
         sp = zs[ai]
         N, K, S = self.n_max, self.K, self.S
         r2 = (rv * rv).sum(1)
-        B, Bh = radial_B_Bhat(r2, self.betas, self.gamma, self.pref)
+        B, Bh = self.radial(r2)
         R, dR = solid_harmonics(rv, self.l_max, gradients=True)
         Bl, Bhl = B[:, :, self.l_of_lm], Bh[:, :, self.l_of_lm]
         c = np.zeros((A * S, N * K))

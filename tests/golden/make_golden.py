@@ -21,7 +21,18 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 
 
-def main(ref_src: str) -> None:
+POLY_W_CASES = {
+    # name: extra constructor arguments on top of the 192-atom cluster's parameters
+    "poly": {"rbf": "polynomial"},
+    "w_pow": {"weighting": {"function": "pow", "r0": 2.0, "c": 1.0, "d": 1.0, "m": 1.0, "w0": 0.5}},
+    "w_poly": {"weighting": {"function": "poly", "r0": 4.0, "c": 1.0, "m": 2.0}},
+    "w_exp": {"weighting": {"function": "exp", "r0": 1.5, "c": 1.0, "d": 0.5}},
+    "w_w0": {"weighting": {"w0": 0.0}},
+    "poly_w_pow": {"rbf": "polynomial", "weighting": {"function": "pow", "r0": 2.0, "c": 1.0, "d": 1.0, "m": 2.0}},
+}
+
+
+def main(ref_src: str, groups=("G1", "G2", "G3", "G4")) -> None:
     sys.path.insert(0, os.path.join(ROOT, "oracle", "sphericart_shim"))
     sys.path.insert(0, ref_src)
     sys.path.insert(1, ROOT)
@@ -32,6 +43,11 @@ def main(ref_src: str) -> None:
 
     def ref(**kw):
         return SOAP(dtype="float64", device="cpu", **kw)
+
+    if "G4" in groups:
+        make_poly_weighting(ref, W)
+    if "G1" not in groups and "G2" not in groups and "G3" not in groups:
+        return
 
     # --- G1: 192-atom water cluster, the CPU workload's parameters --------
     s = W.make("cluster192")
@@ -105,5 +121,42 @@ def main(ref_src: str) -> None:
     print("golden fixtures written to", HERE)
 
 
+def make_poly_weighting(ref, W) -> None:
+    """G4: polynomial radial basis and weighting functions on the 192-atom
+    cluster: create() (off and cc) and the reference's analytical derivatives
+    (its closed form for rbf='polynomial', its autograd path with weighting);
+    plus r_cut inferred from a weighting and a heavier polynomial basis
+    (n_max 6, l_max 6, sigma 1) on a small periodic water box."""
+    s = W.make("cluster192")
+    P = dict(W.CONFIGS["cluster192"])
+    centers, include = [0, 7, 100], list(range(40))
+    out = {"positions": s["positions"], "Z": s["atomic_numbers"], "centers": np.array(centers),
+           "include": np.array(include)}
+    for name, extra in POLY_W_CASES.items():
+        soap = ref(**{**P, **extra})
+        out[f"{name}_create"] = soap.create(s).numpy()[:48]  # first 48 centres kept (fixture size)
+        out[f"{name}_cc"] = ref(**{**P, **extra, "average": "cc"}).create(s).numpy()[:48]
+        J = soap.derivatives(s, centers=centers, include=include, method="analytical", return_descriptor=False)
+        out[f"{name}_deriv"] = J.numpy()
+    # r_cut from the weighting (pow: r0 (c/threshold - d)^(1/m))
+    wt = {"function": "pow", "r0": 0.5, "c": 1.0, "d": 1.0, "m": 2.0, "threshold": 1e-2}
+    Pn = {k: v for k, v in P.items() if k != "r_cut"}
+    soap = ref(**Pn, r_cut=None, weighting=wt)
+    out["infer_rcut"] = np.array(soap._r_cut)
+    out["infer_create"] = soap.create(s).numpy()[:48]
+    np.savez_compressed(os.path.join(HERE, "poly_weighting.npz"), **out)
+    # heavier polynomial basis on a small periodic box
+    box = W.water_box(8, 6.21, seed=5, dmin=2.4)
+    Pb = {"species": [1, 8], "r_cut": 5.0, "n_max": 6, "l_max": 6, "sigma": 1.0, "rbf": "polynomial",
+          "periodic": True}
+    soap = ref(**Pb)
+    sysb = {"positions": box["positions"], "atomic_numbers": box["atomic_numbers"], "cell": box["cell"],
+            "pbc": box["pbc"]}
+    outb = {"positions": box["positions"], "Z": box["atomic_numbers"], "cell": box["cell"],
+            "create": soap.create(sysb, centers=[0, 1, 2, 3]).numpy()}
+    np.savez_compressed(os.path.join(HERE, "poly_box.npz"), **outb)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src",
+         tuple(sys.argv[2:]) if len(sys.argv) > 2 else ("G1", "G2", "G3", "G4"))

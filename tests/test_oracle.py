@@ -171,3 +171,59 @@ def test_pbc_offsets_cover_cutoff():
     assert off.shape == (125, 3)
     off = pbc_offsets(cell, [True, False, True], 7.487)
     assert off.shape == (25, 3)
+
+
+# ---- polynomial radial basis and weighting functions (golden group G4) ----
+
+POLY_W_CASES = {
+    "poly": {"rbf": "polynomial"},
+    "w_pow": {"weighting": {"function": "pow", "r0": 2.0, "c": 1.0, "d": 1.0, "m": 1.0, "w0": 0.5}},
+    "w_poly": {"weighting": {"function": "poly", "r0": 4.0, "c": 1.0, "m": 2.0}},
+    "w_exp": {"weighting": {"function": "exp", "r0": 1.5, "c": 1.0, "d": 0.5}},
+    "w_w0": {"weighting": {"w0": 0.0}},
+    "poly_w_pow": {"rbf": "polynomial", "weighting": {"function": "pow", "r0": 2.0, "c": 1.0, "d": 1.0, "m": 2.0}},
+}
+
+
+@pytest.mark.parametrize("name", list(POLY_W_CASES))
+def test_poly_and_weighting_match_reference(golden, name):
+    """create (ps and cc) and the analytical derivatives; with weighting the
+    reference differentiates by autograd, the oracle in closed form."""
+    g = golden("poly_weighting")
+    extra = POLY_W_CASES[name]
+    pos, Z = g["positions"], g["Z"]
+    o = _cfg("cluster192", **extra)
+    assert rel_l2(o.create(pos, Z)[:48], g[f"{name}_create"]) < TOL
+    assert rel_l2(_cfg("cluster192", average="cc", **extra).create(pos, Z)[:48], g[f"{name}_cc"]) < TOL
+    J = o.derivatives(pos, Z, centers=list(g["centers"]), include=list(g["include"]), return_descriptor=False)
+    assert rel_l2(J, g[f"{name}_deriv"]) < TOL
+
+
+def test_rcut_inferred_from_weighting(golden):
+    g = golden("poly_weighting")
+    P = {k: v for k, v in W.CONFIGS["cluster192"].items() if k != "r_cut"}
+    o = OracleSOAP(**P, r_cut=None,
+                   weighting={"function": "pow", "r0": 0.5, "c": 1.0, "d": 1.0, "m": 2.0, "threshold": 1e-2})
+    assert abs(o.r_cut - float(g["infer_rcut"])) < 1e-12
+    assert rel_l2(o.create(g["positions"], g["Z"])[:48], g["infer_create"]) < TOL
+
+
+def test_poly_basis_periodic_box(golden):
+    g = golden("poly_box")
+    o = OracleSOAP(species=[1, 8], r_cut=5.0, n_max=6, l_max=6, sigma=1.0, rbf="polynomial", periodic=True)
+    d = o.create(g["positions"], g["Z"], centers=[0, 1, 2, 3], cell=g["cell"], pbc=[True] * 3)
+    assert rel_l2(d, g["create"]) < 1e-10
+
+
+def test_weighting_derivative_is_the_slope():
+    """The closed-form dw/dr equals a central difference of w(r)."""
+    from oracle.soap_oracle import Weighting
+    r = np.linspace(0.3, 6.0, 57)
+    for kw in ({"function": "pow", "r0": 2.0, "c": 1.0, "d": 1.0, "m": 1.5},
+               {"function": "poly", "r0": 4.5, "c": 2.0, "m": 3.0},
+               {"function": "exp", "r0": 1.5, "c": 1.0, "d": 0.5}):
+        w = Weighting(**kw)
+        _, dw = w.value_and_derivative(r)
+        h = 1e-6
+        fd = (w.value_and_derivative(r + h)[0] - w.value_and_derivative(r - h)[0]) / (2 * h)
+        assert np.allclose(dw, fd, rtol=1e-6, atol=1e-9), kw
