@@ -14,6 +14,8 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsoapb200
 OK, ERR_ARG, ERR_CUDA, ERR_CAPACITY, ERR_UNSUPPORTED, ERR_ACCURACY = range(6)
 OUT_PS, OUT_CC, OUT_RAW = 0, 1, 2
 NL_CREATE, NL_ALL = 0, 1
+RBF_GTO, RBF_POLY = 0, 1
+W_NONE, W_W0, W_POLY, W_POW, W_EXP = range(5)
 
 # Every symbol include/soapb200.h declares (checked by the CPU test suite).
 EXPORTS = (
@@ -29,12 +31,15 @@ class Basis(ctypes.Structure):
     _fields_ = [
         ("n_max", c_int32), ("l_max", c_int32), ("n_species", c_int32), ("crossover", c_int32),
         ("r_cut", c_double), ("sigma", c_double),
+        ("rbf", c_int32), ("weighting", c_int32),
+        ("w_r0", c_double), ("w_c", c_double), ("w_d", c_double), ("w_m", c_double), ("w_w0", c_double),
+        ("quad_n", c_int32), ("seg_hint", c_int32), ("h_poly", c_void_p),
         ("eta", c_double), ("cutoff", c_double), ("seg_width", c_double),
         ("n_seg", c_int32), ("n_keys", c_int32), ("n_feat_ps", c_int32), ("n_feat_cc", c_int32),
         ("bytes", c_int64),
         ("off_alpha", c_int64), ("off_beta", c_int64), ("off_tab_b", c_int64), ("off_tab_bh", c_int64),
         ("off_ftab", c_int64), ("off_widx", c_int64), ("off_err", c_int64),
-        ("off_tabt_b", c_int64), ("off_tabt_bh", c_int64),
+        ("off_tabt_b", c_int64), ("off_tabt_bh", c_int64), ("off_self", c_int64), ("off_poly", c_int64),
         ("dev", c_void_p),
     ]
 

@@ -29,6 +29,7 @@ struct DescArgs {
   const float4* pairs;
   int64_t n_centres;
   const float* tab_b;
+  const float* selfv;  // w0 B_nl(0): value of r = 0 edges (the centre's own Gaussian)
   float* out;
   float* coeff_out;  // optional raw c[s][n][lm] rows (S N K floats per centre)
   int* counter;
@@ -89,6 +90,12 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
   const bool active = l_me <= L && k_me * GN < N;
   const int lme = active ? l_me : 0;
   const int mme = 2 * lme + 1;
+  float selfb[GN];
+#pragma unroll
+  for (int g = 0; g < GN; ++g) {
+    const int n = k_me * GN + g;
+    selfb[g] = (active && n < N) ? __ldg(a.selfv + fn_index(n, lme, N)) : 0.0f;
+  }
 
   for (;;) {
     int c32 = 0;
@@ -138,7 +145,7 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
         int seg;
         float t;
         seg_coord(r, a.inv_h, a.nseg, seg, t);
-        tt[lane] = t;
+        tt[lane] = (r > 0.0f) ? t : 3.0f;  // 3: r = 0 edge, takes the self value
         sg[lane] = seg;
         spp[lane] = (int)((unsigned)w >> kAtomBits);
         float* yrow = Y + lane * YS;
@@ -165,7 +172,7 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
         const float t = tt[q];
         float B[GN];
 #pragma unroll
-        for (int g = 0; g < GN; ++g) B[g] = horner7(cf[g], t);
+        for (int g = 0; g < GN; ++g) B[g] = (t > 2.0f) ? selfb[g] : horner7(cf[g], t);
         const float* yr = Y + q * YS + lme * lme;
 #pragma unroll
         for (int m = 0; m < M; ++m) {
@@ -301,6 +308,7 @@ extern "C" int soapb_descriptor(const soapb_basis* b, int64_t n_centres, const i
   a.pairs = (const float4*)d_pairs;
   a.n_centres = n_centres;
   a.tab_b = (const float*)((const char*)b->dev + b->off_tab_b);
+  a.selfv = (const float*)((const char*)b->dev + b->off_self);
   a.out = d_out;
   a.coeff_out = d_coeff;
   a.counter = d_counter;

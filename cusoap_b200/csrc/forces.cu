@@ -39,7 +39,8 @@ struct ForceArgs {
   const float* dEdp;
   const int* centre_atom;
   const float* tabt_b;   // [fn][seg][8]
-  const float* tabt_bh;
+  const float* tabt_bh;  // D = d(w B)/dr; Bhat = D / r
+  const float* selfv;    // w0 B_nl(0) for r = 0 edges
   const int* widx;
   float* G;              // (n_centres, S N K) workspace
   float* forces;
@@ -148,7 +149,10 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
       const float x = pr.x, y = pr.y, z = pr.z;
       int seg;
       float t;
-      seg_coord(sqrtf(x * x + y * y + z * z), a.inv_h, nseg, seg, t);
+      const float r = sqrtf(x * x + y * y + z * z);
+      seg_coord(r, a.inv_h, nseg, seg, t);
+      const bool self_edge = !(r > 0.0f);
+      const float inv_r = self_edge ? 0.0f : 1.0f / r;
       const EdgeHarmonics<L> eh(x, y, z);
       const float* gs = G + sp * N * KC;
       float ex = 0.f, ey = 0.f, ez = 0.f;
@@ -162,7 +166,7 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
           float cf[kNCoef], ch[kNCoef];
           load_coef(a.tabt_b, fn, seg, nseg, cf);   // function-major: row fn, column seg
           load_coef(a.tabt_bh, fn, seg, nseg, ch);
-          const float b = horner7(cf, t), h = horner7(ch, t);
+          const float b = self_edge ? __ldg(a.selfv + fn) : horner7(cf, t), h = horner7(ch, t) * inv_r;
           const float* gr = gs + n * KC + l * l;
 #pragma unroll
           for (int m = 0; m < 2 * l + 1; ++m) {
@@ -321,6 +325,7 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.centre_atom = d_centre_atom;
   a.tabt_b = (const float*)((const char*)b->dev + b->off_tabt_b);
   a.tabt_bh = (const float*)((const char*)b->dev + b->off_tabt_bh);
+  a.selfv = (const float*)((const char*)b->dev + b->off_self);
   a.widx = (const int*)((const char*)b->dev + b->off_widx);
   a.G = (float*)d_work;
   a.forces = d_forces;

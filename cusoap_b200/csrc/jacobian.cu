@@ -47,7 +47,8 @@ struct JacArgs {
   const int* inc_row;
   const int* centre_atom;
   const float* tab_b;
-  const float* tab_bh;
+  const float* tab_bh;   // D = d(w B)/dr; Bhat = D / r
+  const float* selfv;    // w0 B_nl(0) for r = 0 edges
   const int* ftab;
   float* out;
   int* status;
@@ -235,9 +236,9 @@ __device__ void stage_entries(const JacArgs& a, int64_t p0, const unsigned long 
       seg_coord(r, a.inv_h, a.nseg, seg, tt);
       float cf[kNCoef];
       load_coef(a.tab_b, seg, fn, NF, cf);
-      h[8 + fn] = horner7(cf, tt);
+      h[8 + fn] = (r > 0.0f) ? horner7(cf, tt) : __ldg(a.selfv + fn);
       load_coef(a.tab_bh, seg, fn, NF, cf);
-      h[8 + NF + fn] = horner7(cf, tt);
+      h[8 + NF + fn] = (r > 0.0f) ? horner7(cf, tt) / r : 0.0f;
     }
   } else if (NF > nth) {  // more radial functions than threads: flat loop
     for (int t = tid; t < nb * NF; t += nth) {
@@ -249,9 +250,9 @@ __device__ void stage_entries(const JacArgs& a, int64_t p0, const unsigned long 
       seg_coord(r, a.inv_h, a.nseg, seg, tt);
       float cf[kNCoef];
       load_coef(a.tab_b, seg, fn, NF, cf);
-      h[8 + fn] = horner7(cf, tt);
+      h[8 + fn] = (r > 0.0f) ? horner7(cf, tt) : __ldg(a.selfv + fn);
       load_coef(a.tab_bh, seg, fn, NF, cf);
-      h[8 + NF + fn] = horner7(cf, tt);
+      h[8 + NF + fn] = (r > 0.0f) ? horner7(cf, tt) / r : 0.0f;
     }
   }
   compute_bar(nth);
@@ -552,6 +553,7 @@ extern "C" int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int
   a.centre_atom = d_centre_atom;
   a.tab_b = (const float*)((const char*)b->dev + b->off_tab_b);
   a.tab_bh = (const float*)((const char*)b->dev + b->off_tab_bh);
+  a.selfv = (const float*)((const char*)b->dev + b->off_self);
   a.ftab = (const int*)((const char*)b->dev + b->off_ftab);
   a.out = d_out;
   a.status = d_status;

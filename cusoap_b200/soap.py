@@ -17,8 +17,12 @@ Differences from the reference, by design:
   ``requires_grad``: the backward pass is a hand-written adjoint kernel
   (the reference reaches the same gradient only through autograd);
 * ``derivatives`` uses the closed-form Jacobian kernel for every case it
-  supports (periodic systems and ``attach=True`` included), where the
-  reference falls back to a batched-autograd Jacobian (SG:2677-2698).
+  supports (periodic systems, weighting and ``attach=True`` included), where
+  the reference falls back to a batched-autograd Jacobian (SG:2677-2698);
+* the polynomial basis's radial integrals are evaluated with an accurate
+  series / recurrence split of the scaled Bessel functions when the tables
+  are built; the reference's clamped upward recurrence differs from it for
+  high l at small r (t = 2 eta rx r < l).
 """
 from __future__ import annotations
 
@@ -54,6 +58,60 @@ def _resolve_z(s) -> int:
                 return _SYMBOLS[s]
             raise ValueError(f"Cannot resolve species symbol '{s}'. Install ASE or use atomic numbers.")
     return int(s)
+
+
+class _Weighting:
+    """DScribe weighting parameters (SG:403-470); the functions themselves
+    are evaluated on the device when the radial tables are built."""
+
+    def __init__(self, function: Optional[str] = None, r0: float = 1.0, c: float = 1.0, d: float = 1.0,
+                 m: float = 1.0, w0: float = 1.0):
+        if function not in (None, "poly", "pow", "exp"):
+            raise ValueError(f"Unknown weighting function: {function}")
+        self.function, self.r0, self.c, self.d, self.m, self.w0 = function, float(r0), float(c), float(d), \
+            float(m), float(w0)
+
+    def infer_rcut(self, threshold: float = 1e-2) -> float:
+        """r_cut where the weight falls to `threshold` (SG:422-438)."""
+        if self.function is None:
+            raise ValueError("Cannot infer r_cut when weighting.function is None; provide r_cut explicitly.")
+        if self.function == "poly":
+            return self.r0
+        val = self.c / threshold - self.d
+        if val <= 0:
+            raise ValueError(f"Invalid weighting: c/threshold - d must be >0 for {self.function}.")
+        if self.function == "pow":
+            return self.r0 * val ** (1.0 / self.m)
+        return -self.r0 * math.log(val)
+
+
+def _poly_grid(r_cut: float, n_max: int, quad_n: int) -> np.ndarray:
+    """DScribe polynomial basis on its Gauss-Legendre grid: rx | wr | g_n(rx),
+    float64, with g = sqrtm(inv(S)) (r_cut - rx)^(k+2) computed as the
+    reference does it (SG:710-752, nodes by Golub-Welsch SG:350-362).  The
+    overlap S is so ill-conditioned that only this exact sequence of FP64
+    operations reproduces the reference's basis; it runs once per SOAP object
+    on the host, like the reference's own set-up."""
+    from scipy.linalg import sqrtm
+    n, rc = int(n_max), float(r_cut)
+    S = np.zeros((n, n))
+    for i in range(1, n + 1):
+        for j in range(1, n + 1):
+            S[i - 1, j - 1] = (2 * rc ** (7 + i + j)) / ((5 + i + j) * (6 + i + j) * (7 + i + j))
+    betas = sqrtm(np.linalg.inv(S))
+    if np.iscomplexobj(betas):
+        raise ValueError("Could not calculate normalization factors for the radial basis in the domain of real "
+                         "numbers. Lowering the number of radial basis functions (n_max) or increasing the radial "
+                         "cutoff (r_cut) is advised.")
+    k = np.arange(1, quad_n, dtype=np.float64)
+    beta = k / np.sqrt(4.0 * k * k - 1.0)
+    x, V = np.linalg.eigh(np.diag(beta, 1) + np.diag(beta, -1))
+    w = 2.0 * V[0, :] ** 2
+    rx = rc * 0.5 * (x + 1.0)
+    wr = rc * 0.5 * w
+    fs = np.stack([(rc - np.clip(rx, 0.0, rc)) ** (kk + 2) for kk in range(1, n + 1)])
+    g = np.ascontiguousarray(betas) @ fs
+    return np.ascontiguousarray(np.concatenate([rx, wr, g.reshape(-1)]), dtype=np.float64)
 
 
 class _Batch:
@@ -225,39 +283,67 @@ class SOAP:
             raise ValueError("average must be one of: 'off', 'inner', 'outer', 'cc' (cc = projection coeffs).")
         if self._rbf not in ("gto", "polynomial"):
             raise ValueError("rbf must be 'gto' or 'polynomial'.")
-        if self._rbf != "gto":
-            raise NotImplementedError("rbf='polynomial' is not built in this library yet (gto only)")
-        if weighting is not None:
-            raise NotImplementedError("weighting functions are not built in this library yet")
+        # weighting dict as DScribe's: may carry 'threshold' for the r_cut inference (SG:584-597)
+        self._weighting_dict = dict(weighting) if weighting is not None else None
+        self._weighting = None
+        thr = 1e-2
+        if self._weighting_dict is not None:
+            thr = float(self._weighting_dict.get("threshold", 1e-2))
+            self._weighting = _Weighting(**{k: v for k, v in self._weighting_dict.items() if k != "threshold"})
         if r_cut is None:
-            raise ValueError("Either r_cut or weighting must be provided.")
-        self._r_cut = float(r_cut)
+            if self._weighting is None:
+                raise ValueError("Either r_cut or weighting must be provided.")
+            self._r_cut = float(self._weighting.infer_rcut(thr))
+        else:
+            self._r_cut = float(r_cut)
         self._cutoff_padding = float(self._sigma * math.sqrt(-2.0 * math.log(1e-3)))  # SG:600-602
         self._cutoff = self._r_cut + self._cutoff_padding
-
-        lib = _lib.load()
-        self._basis = Basis()
-        self._basis.n_max, self._basis.l_max = self._n_max, self._l_max
-        self._basis.n_species, self._basis.crossover = self.n_species, int(self.crossover)
-        self._basis.r_cut, self._basis.sigma = self._r_cut, self._sigma
-        check(lib.soapb_basis_plan(ctypes.byref(self._basis)))
-        with torch.cuda.device(self.device):
-            self._basis_buf = torch.empty(int(self._basis.bytes), dtype=torch.uint8, device=self.device)
-            check(lib.soapb_basis_build(ctypes.byref(self._basis), _ptr(self._basis_buf), _stream(self.device)))
-            L1, N = self._l_max + 1, self._n_max
-            self._alphas = np.zeros((L1, N))
-            self._betas = np.zeros((L1, N, N))
-            err = np.zeros(2)
-            check(lib.soapb_basis_download(ctypes.byref(self._basis), self._alphas.ctypes.data,
-                                           self._betas.ctypes.data, err.ctypes.data, _stream(self.device)))
-        self.table_error = (float(err[0]), float(err[1]))
-        if max(self.table_error) > 1e-6:
-            raise _lib.SoapbError(_lib.ERR_ACCURACY, f"radial table error {self.table_error} above 1e-6")
+        self._poly_grid = _poly_grid(self._r_cut, self._n_max, self.quad_n) if self._rbf == "polynomial" else None
+        self._build_basis()
         self._counter = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.n_features = int(self.get_number_of_features())
         # When a list, every library call appends (name, start_event, end_event)
         # recorded on the launch stream (per-stage GPU timing).
         self.profile: Optional[list] = None
+
+    def _build_basis(self):
+        """Plan and build the basis on the device; tables whose error exceeds
+        1e-6 are rebuilt on finer segments (weighting functions with a sharp
+        feature need them)."""
+        lib = _lib.load()
+        w = self._weighting
+        seg_hint = 0
+        while True:
+            b = Basis()
+            b.n_max, b.l_max, b.n_species, b.crossover = self._n_max, self._l_max, self.n_species, int(self.crossover)
+            b.r_cut, b.sigma = self._r_cut, self._sigma
+            b.rbf = _lib.RBF_POLY if self._rbf == "polynomial" else _lib.RBF_GTO
+            if w is None:
+                b.weighting = _lib.W_NONE
+            else:
+                b.weighting = {None: _lib.W_W0, "poly": _lib.W_POLY, "pow": _lib.W_POW, "exp": _lib.W_EXP}[w.function]
+                b.w_r0, b.w_c, b.w_d, b.w_m, b.w_w0 = w.r0, w.c, w.d, w.m, w.w0
+            if self._poly_grid is not None:
+                b.quad_n = self.quad_n
+                b.h_poly = self._poly_grid.ctypes.data
+            b.seg_hint = seg_hint
+            check(lib.soapb_basis_plan(ctypes.byref(b)))
+            with torch.cuda.device(self.device):
+                buf = torch.empty(int(b.bytes), dtype=torch.uint8, device=self.device)
+                check(lib.soapb_basis_build(ctypes.byref(b), _ptr(buf), _stream(self.device)))
+                L1, N = self._l_max + 1, self._n_max
+                alphas, betas, err = np.zeros((L1, N)), np.zeros((L1, N, N)), np.zeros(2)
+                check(lib.soapb_basis_download(ctypes.byref(b), alphas.ctypes.data, betas.ctypes.data,
+                                               err.ctypes.data, _stream(self.device)))
+            self.table_error = (float(err[0]), float(err[1]))
+            if max(self.table_error) <= 1e-6:
+                break
+            if (2 * b.n_seg) * self.n_species > 1024:
+                raise _lib.SoapbError(_lib.ERR_ACCURACY, f"radial table error {self.table_error} above 1e-6 "
+                                      f"with {b.n_seg} segments (weighting too sharp for the FP32 tables)")
+            seg_hint = 2 * b.n_seg
+        self._basis, self._basis_buf = b, buf
+        self._alphas, self._betas = alphas, betas
 
     def _call(self, name, fn, *args):
         prof = self.profile

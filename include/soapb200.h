@@ -49,34 +49,65 @@ enum {
   SOAPB_OUT_RAW = 2  /* c[s][n][lm] per centre, no permutation / scaling */
 };
 
-/* GTO basis + radial tables.  Fill the five input fields, call
+/* radial basis functions (SOAP rbf argument, SG:616-621) */
+enum {
+  SOAPB_RBF_GTO = 0,  /* Gaussian-type orbitals, Loewdin-orthonormalised (SG:690-708) */
+  SOAPB_RBF_POLY = 1  /* DScribe polynomials (r_cut - r)^(k+2), orthonormalised by the caller (SG:710-752) */
+};
+
+/* weighting of the neighbour densities (SOAP weighting argument, SG:403-470) */
+enum {
+  SOAPB_W_NONE = 0,  /* no weighting: w = 1, w0 = 1 */
+  SOAPB_W_W0 = 1,    /* function None: w = 1 for r > 0, w0 = w_w0 for the centre's own Gaussian */
+  SOAPB_W_POLY = 2,  /* w = c (1 + 2 x^3 - 3 x^2)^m for x = r / r0 <= 1, else 0 */
+  SOAPB_W_POW = 3,   /* w = c / (d + x^m) */
+  SOAPB_W_EXP = 4    /* w = c / (d + exp(-r / r0)) */
+};
+
+/* Radial basis + radial tables.  Fill the input fields, call
  * soapb_basis_plan (host only) to get the sizes, allocate `bytes` of device
  * memory, then soapb_basis_build.  Replaces SOAP.__init__'s basis set-up:
- * _init_gto_basis SG:690-708, _lowdin_invsqrt SG:339-343, the cutoff
- * padding SG:600-602 and the feature tables SG:1215-1291. */
+ * _init_gto_basis SG:690-708, _lowdin_invsqrt SG:339-343, _init_poly_basis
+ * SG:710-752, the weighting SG:403-470 / SG:584-597, the self terms
+ * SG:765-819, the cutoff padding SG:600-602 and the feature tables
+ * SG:1215-1291.
+ *
+ * Radial tables: for every radial function (n, l) and segment, degree-7
+ * polynomials in the segment coordinate t in [-1, 1] of
+ *   B(r) = w(r) B_nl(r)            (c_nlm of an edge = B(r) R_lm(rvec))
+ *   D(r) = d/dr [w(r) B_nl(r)]     (d c_nlm / d rvec = rvec D / r R_lm + B grad R_lm)
+ * built in FP64 on the device.  Edges at r = 0 (the centre's own Gaussian)
+ * use the per-function self value w0 B_nl(0) instead of the table. */
 typedef struct soapb_basis {
   /* inputs */
   int32_t n_max, l_max, n_species, crossover;
   double r_cut, sigma;
+  int32_t rbf;          /* SOAPB_RBF_* */
+  int32_t weighting;    /* SOAPB_W_* */
+  double w_r0, w_c, w_d, w_m, w_w0;  /* weighting parameters (DScribe names) */
+  int32_t quad_n;       /* SOAPB_RBF_POLY: Gauss-Legendre points of the caller's grid */
+  int32_t seg_hint;     /* 0, or a lower bound on n_seg (finer tables) */
+  const double* h_poly; /* SOAPB_RBF_POLY: host rx[quad_n] | wr[quad_n] | g[n_max][quad_n] (g_n on the grid) */
   /* derived by soapb_basis_plan */
   double eta;        /* 1 / (2 sigma^2) */
   double cutoff;     /* r_cut + sigma sqrt(-2 ln 1e-3) */
-  double seg_width;  /* radial table segment width (A) */
-  int32_t n_seg;     /* radial table segments over [0, cutoff] */
+  double seg_width;  /* radial table segment width (A); n_seg * seg_width >= cutoff */
+  int32_t n_seg;     /* radial table segments */
   int32_t n_keys;    /* n_species * n_seg: neighbour sort keys */
   int32_t n_feat_ps; /* SG:913-919 */
   int32_t n_feat_cc; /* SG:909-910 */
   int64_t bytes;     /* device bytes the basis needs */
   int64_t off_alpha, off_beta, off_tab_b, off_tab_bh, off_ftab, off_widx, off_err;  /* byte offsets into dev */
   int64_t off_tabt_b, off_tabt_bh; /* function-major copies of the radial tables */
+  int64_t off_self, off_poly;      /* self values (n_max (l_max+1) float); device copy of h_poly */
   void* dev;         /* set by soapb_basis_build */
 } soapb_basis;
 
 int soapb_basis_plan(soapb_basis* b);
 int soapb_basis_build(soapb_basis* b, void* dev_buf, void* stream);
-/* Copy the FP64 alpha (l_max+1, n_max), beta (l_max+1, n_max, n_max) and the
- * two table errors (max |table - exact| / max|exact| for B and Bhat) to host
- * memory; synchronises the stream. */
+/* Copy the FP64 alpha (l_max+1, n_max), beta (l_max+1, n_max, n_max) (GTO
+ * only) and the two table errors (max |table - exact| / max|exact| per
+ * function for B and D) to host memory; synchronises the stream. */
 int soapb_basis_download(const soapb_basis* b, double* h_alpha, double* h_beta, double* h_err2, void* stream);
 
 /* A batch of structures.  Atoms of structure i are [atom_off[i], atom_off[i+1]).

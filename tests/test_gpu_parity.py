@@ -44,7 +44,8 @@ def test_basis_and_tables():
     o = _oracle("cells512")
     assert rel_l2(s._alphas, o.alphas) < 1e-14
     assert rel_l2(s._betas, o.betas) < 1e-8
-    assert max(s.table_error) < 1e-7
+    # B and D = d(wB)/dr tables, relative to each function's maximum (the constructor enforces 1e-6)
+    assert max(s.table_error) < 5e-7
 
 
 @pytest.mark.parametrize("avg", ["off", "inner", "outer", "cc"])
