@@ -42,11 +42,12 @@ struct ForceArgs {
   const float* tabt_bh;  // D = d(w B)/dr; Bhat = D / r
   const float* selfv;    // w0 B_nl(0) for r = 0 edges
   const int* widx;
+  const int* ftab;       // second half: l-major pair indices of every feature
   float* G;              // (n_centres, S N K) workspace
   float* forces;
   int* counter;
   int64_t n_centres;
-  int N, S, nseg, F, attach;
+  int N, S, nseg, F, attach, crossover;
   float inv_h;
 };
 
@@ -91,6 +92,76 @@ __global__ void __launch_bounds__(kGThreads) k_adjoint_g(ForceArgs a) {
 #pragma unroll
       for (int m = 0; m < 2 * L + 1; ++m)
         if (m < 2 * l + 1) grow[ai * K + l * l + m] = pref * g[m];
+    }
+    __syncthreads();
+  }
+}
+
+// G = dE/dc for one centre per block iteration, W dense in shared memory:
+// the dE/dp row is scattered into W_l[a][b] (both triangles, 2x on a = b,
+// times pref_l) through the l-major pair table, then G[a, lm] = sum_b
+// W_l[a][b] c[b, lm] with lanes over a (W rows padded to SN + 1 floats:
+// conflict-free) and c broadcast.  Used while (L+1) SN (SN+1) floats fit.
+// One G task (a, l) with l known at compile time: G[a, l^2 .. l^2 + 2l] = sum_b W_l[a][b] c[b, lm].
+template <int L, int l>
+__device__ __forceinline__ void g_task(const float* Wr, const float* s_c, int SN, float* grow) {
+  constexpr int K = (L + 1) * (L + 1), KC = K | 1, M = 2 * l + 1;
+  float g[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) g[m] = 0.0f;
+#pragma unroll 4
+  for (int bi = 0; bi < SN; ++bi) {
+    const float w = Wr[bi];
+    const float* cr = s_c + bi * KC + l * l;
+#pragma unroll
+    for (int m = 0; m < M; ++m) g[m] = fmaf(w, cr[m], g[m]);
+  }
+#pragma unroll
+  for (int m = 0; m < M; ++m) grow[l * l + m] = g[m];
+}
+
+template <int L, int l = 0>
+__device__ __forceinline__ void g_task_l(int lr, const float* Wr, const float* s_c, int SN, float* grow) {
+  if constexpr (l <= L) {
+    if (lr == l) g_task<L, l>(Wr, s_c, SN, grow);
+    else g_task_l<L, l + 1>(lr, Wr, s_c, SN, grow);
+  }
+}
+
+template <int L>
+__global__ void __launch_bounds__(kGThreads) k_adjoint_g_dense(ForceArgs a) {
+  constexpr int K = (L + 1) * (L + 1), KC = K | 1;
+  extern __shared__ __align__(16) float sm[];
+  const int N = a.N, S = a.S, SN = S * N, WS = SN + 1, F = a.F;
+  float* s_c = sm;                              // SN x KC
+  float* s_W = sm + ((SN * KC + 3) & ~3);       // (L+1) x SN x WS
+  const int wn = (L + 1) * SN * WS;
+  for (int64_t c = blockIdx.x; c < a.n_centres; c += gridDim.x) {
+    const float* wrow = a.dEdp + (size_t)c * F;
+    const float* crow = a.coeff + (size_t)c * SN * K;
+    for (int i = threadIdx.x; i < SN * K; i += blockDim.x) s_c[(i / K) * KC + (i % K)] = crow[i];
+    // with crossover every (a, b, l) has a feature and is written below
+    if (!a.crossover)
+      for (int i = threadIdx.x; i < wn; i += blockDim.x) s_W[i] = 0.0f;
+    __syncthreads();
+    for (int f = threadIdx.x; f < F; f += blockDim.x) {
+      const int code = __ldg(a.ftab + F + f);
+      const int l = code >> 24, base = l * SN;
+      const int ia = (code & 0xfff) - base, ib = ((code >> 12) & 0xfff) - base;
+      const float w = wrow[f] * sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * l + 1.0f));
+      float* Wl = s_W + (size_t)l * SN * WS;
+      if (ia == ib) {
+        Wl[ia * WS + ia] = 2.0f * w;
+      } else {
+        Wl[ia * WS + ib] = w;
+        Wl[ib * WS + ia] = w;
+      }
+    }
+    __syncthreads();
+    float* grow = a.G + (size_t)c * SN * K;
+    for (int t = threadIdx.x; t < SN * (L + 1); t += blockDim.x) {
+      const int l = L - t / SN, ai = t % SN;
+      g_task_l<L>(l, s_W + ((size_t)l * SN + ai) * WS, s_c, SN, grow + ai * K);
     }
     __syncthreads();
   }
@@ -252,7 +323,21 @@ struct ForceDispatch {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     // G = dE/dc
-    {
+    const int SN = a.S * a.N;
+    const int64_t dense_bytes = 4 * (int64_t)(((SN * ((L + 1) * (L + 1) | 1) + 3) & ~3) + (L + 1) * SN * (SN + 1));
+    if (dense_bytes <= 100 * 1024) {
+      auto kern = k_adjoint_g_dense<L>;
+      const int smem = (int)dense_bytes;
+      int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                          "adjoint smem attribute");
+      if (rc) return rc;
+      int occ = 1;
+      if ((rc = resident_blocks((const void*)kern, kGThreads, smem, &occ))) return rc;
+      int64_t blocks = (int64_t)nsm * occ;
+      if (blocks > a.n_centres) blocks = a.n_centres;
+      kern<<<(unsigned)blocks, kGThreads, smem, st>>>(a);
+      if ((rc = check_launch("k_adjoint_g_dense"))) return rc;
+    } else {
       const int cbytes = 4 * ((a.S * a.N * ((L + 1) * (L + 1) | 1) + 3) & ~3);
       const bool stage = cbytes + 4 * (int64_t)a.F <= 100 * 1024;
       auto kern = stage ? k_adjoint_g<L, true> : k_adjoint_g<L, false>;
@@ -327,6 +412,7 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.tabt_bh = (const float*)((const char*)b->dev + b->off_tabt_bh);
   a.selfv = (const float*)((const char*)b->dev + b->off_self);
   a.widx = (const int*)((const char*)b->dev + b->off_widx);
+  a.ftab = (const int*)((const char*)b->dev + b->off_ftab);
   a.G = (float*)d_work;
   a.forces = d_forces;
   a.counter = d_counter;
@@ -336,6 +422,7 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.nseg = b->n_seg;
   a.F = b->n_feat_ps;
   a.attach = attach ? 1 : 0;
+  a.crossover = b->crossover ? 1 : 0;
   a.inv_h = (float)(1.0 / b->seg_width);
   int rc = check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st), "reset work counter");
   if (rc) return rc;

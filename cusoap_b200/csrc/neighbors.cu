@@ -242,17 +242,44 @@ __global__ void k_grid_init(soapb_structs s, NLWork w, double cutoff) {
   if (bad && anyp) atomicOr(w.status, 1);
 }
 
+// Fractional bounding box per structure.  Atoms of a structure are
+// contiguous, so a warp usually covers one structure: it reduces min / max
+// with shuffles and issues one atomic per bound instead of 32.
 __global__ void k_frac_bbox(soapb_structs s, NLWork w) {
-  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < s.n_atoms;
-       a += (int64_t)gridDim.x * blockDim.x) {
-    const int si = struct_of_atom(s.d_atom_off, s.n_struct, a);
-    const GridDesc& g = w.grids[si];
-    double f[3];
-    to_frac(g, s.d_positions[3 * a], s.d_positions[3 * a + 1], s.d_positions[3 * a + 2], f);
-    for (int k = 0; k < 3; ++k) {
-      if (g.per[k]) continue;
-      atomicMin(&w.fbox[si * 6 + k], ord_encode(f[k]));
-      atomicMax(&w.fbox[si * 6 + 3 + k], ord_encode(f[k]));
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < s.n_atoms; base += stride) {
+    const int64_t a = base + lane;
+    const bool valid = a < s.n_atoms;
+    int si = 0;
+    double f[3] = {0.0, 0.0, 0.0};
+    if (valid) {
+      si = struct_of_atom(s.d_atom_off, s.n_struct, a);
+      to_frac(w.grids[si], s.d_positions[3 * a], s.d_positions[3 * a + 1], s.d_positions[3 * a + 2], f);
+    }
+    const int si0 = __shfl_sync(0xffffffffu, si, 0);  // lane 0 is always valid here
+    if (__all_sync(0xffffffffu, !valid || si == si0)) {
+      const GridDesc& g = w.grids[si0];
+      for (int k = 0; k < 3; ++k) {
+        if (g.per[k]) continue;
+        double lo = valid ? f[k] : INFINITY, hi = valid ? f[k] : -INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+          hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (lane == 0) {
+          atomicMin(&w.fbox[si0 * 6 + k], ord_encode(lo));
+          atomicMax(&w.fbox[si0 * 6 + 3 + k], ord_encode(hi));
+        }
+      }
+    } else if (valid) {
+      const GridDesc& g = w.grids[si];
+      for (int k = 0; k < 3; ++k) {
+        if (g.per[k]) continue;
+        atomicMin(&w.fbox[si * 6 + k], ord_encode(f[k]));
+        atomicMax(&w.fbox[si * 6 + 3 + k], ord_encode(f[k]));
+      }
     }
   }
 }

@@ -283,3 +283,25 @@ def test_cluster1M_sampled():
     cen = [0, 123_456, 500_000, 1_000_001]
     ref = o.create(sysd["positions"], sysd["atomic_numbers"], centers=cen)
     assert _row_err(_np(out[cen]), ref) < DESC_TOL
+
+
+def test_forces_many_species_vs_oracle():
+    """8 species, n_max 8, l_max 6 (F = 14560): the adjoint's G kernel takes
+    its index-table path (the dense W_l matrices would not fit in shared
+    memory); forces of E = sum w . p against the oracle."""
+    from cusoap_b200 import SOAP
+    rng = np.random.default_rng(11)
+    n = 60
+    pos = rng.uniform(0.0, 9.0, size=(n, 3))
+    Z = rng.choice([1, 2, 3, 4, 5, 6, 7, 8], size=n)
+    Z[:8] = [1, 2, 3, 4, 5, 6, 7, 8]
+    P = dict(species=[1, 2, 3, 4, 5, 6, 7, 8], r_cut=4.0, n_max=8, l_max=6, sigma=0.5)
+    s = SOAP(**P)
+    o = OracleSOAP(**P)
+    w = rng.standard_normal(s.get_number_of_features())
+    pt = torch.tensor(pos, device="cuda", requires_grad=True)
+    E = (s.create({"positions": pt, "atomic_numbers": Z}) * torch.tensor(w, dtype=torch.float32,
+                                                                         device="cuda")).sum()
+    E.backward()
+    Fo = o.forces(pos, Z, np.tile(w, (n, 1)))
+    assert rel_l2(-pt.grad.cpu().numpy(), Fo) < DERIV_TOL
