@@ -521,28 +521,33 @@ __global__ void __launch_bounds__(128) k_count(VisitArgs A, int64_t n_centres, i
   }
 }
 
+constexpr int kFillStage = 512;  // pairs per centre collected in shared memory
+
+// Fill: one warp per centre.  The centre's accepted candidates are collected
+// in shared memory in candidate order (one enumeration), then placed by a
+// stable counting sort on the key (species, radial segment) and written to the
+// centre's CSR slice.  A centre with more than kFillStage pairs enumerates
+// twice instead (histogram, then scatter).  Either way the order is: by key,
+// and by candidate order within a key.
 __global__ void __launch_bounds__(128) k_fill(VisitArgs A, int64_t n_centres, const int64_t* pair_off, float4* pairs,
-                                              int64_t capacity, int nseg, double inv_h, int nkeys, int* status) {
-  extern __shared__ int s_hist[];
+                                              int64_t capacity, int nseg, float inv_h, int nkeys, int* status) {
+  extern __shared__ __align__(16) unsigned char s_raw[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int* hist = s_hist + wid * nkeys;
+  float4* stage = reinterpret_cast<float4*>(s_raw) + (size_t)wid * kFillStage;
+  int* skey = reinterpret_cast<int*>(reinterpret_cast<float4*>(s_raw) + (size_t)(blockDim.x >> 5) * kFillStage) +
+              (size_t)wid * kFillStage;
+  int* hist = reinterpret_cast<int*>(reinterpret_cast<float4*>(s_raw) + (size_t)(blockDim.x >> 5) * kFillStage) +
+              (size_t)(blockDim.x >> 5) * kFillStage + (size_t)wid * nkeys;
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
   if (pair_off[n_centres] > capacity) {
     if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(status, 4);
     return;
   }
-  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid; c < n_centres; c += nw) {
-    for (int k = lane; k < nkeys; k += 32) hist[k] = 0;
-    __syncwarp();
-    auto keyof = [&](int sp, double r2) {
-      const int seg = min((int)(sqrt(r2) * inv_h), nseg - 1);
-      return sp * nseg + seg;
-    };
-    visit(A, c, [&](bool ok, int, int sp, double, double, double, double r2) {
-      if (ok) atomicAdd(&hist[keyof(sp, r2)], 1);
-    });
-    __syncwarp();
-    // exclusive scan of hist (each lane a contiguous chunk)
+  auto keyof = [&](int sp, double r2) {
+    const int seg = min((int)(sqrtf((float)r2) * inv_h), nseg - 1);
+    return sp * nseg + seg;
+  };
+  auto scan_hist = [&]() {  // exclusive scan of hist (each lane a contiguous chunk)
     const int per = (nkeys + 31) / 32;
     const int k0 = min(lane * per, nkeys), k1 = min(k0 + per, nkeys);
     int sum = 0;
@@ -560,20 +565,65 @@ __global__ void __launch_bounds__(128) k_fill(VisitArgs A, int64_t n_centres, co
       run += v;
     }
     __syncwarp();
+  };
+  for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid; c < n_centres; c += nw) {
+    for (int k = lane; k < nkeys; k += 32) hist[k] = 0;
     const int64_t base = pair_off[c];
-    visit(A, c, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double r2) {
-      const int key = ok ? keyof(sp, r2) : -1 - lane;
-      const unsigned peers = __match_any_sync(0xffffffffu, key);
-      const int rank = __popc(peers & ((1u << lane) - 1u));
-      const int start = ok ? hist[key] : 0;
+    const int64_t P = pair_off[c + 1] - base;
+    __syncwarp();
+    if (P <= kFillStage) {
+      int n = 0;
+      visit(A, c, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double r2) {
+        const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+          const int pos = n + __popc(bal & ((1u << lane) - 1u));
+          if (pos < kFillStage) {
+            const int key = keyof(sp, r2);
+            stage[pos] = make_float4((float)rx, (float)ry, (float)rz, __int_as_float(atom | (sp << kAtomBits)));
+            skey[pos] = key;
+            atomicAdd(&hist[key], 1);
+          }
+        }
+        n += __popc(bal);
+      });
       __syncwarp();
-      if (ok) {
-        pairs[base + start + rank] =
-            make_float4((float)rx, (float)ry, (float)rz, __int_as_float(atom | (sp << kAtomBits)));
-        if (rank == 0) hist[key] = start + __popc(peers);
+      scan_hist();
+      const int m = min(n, kFillStage);
+      for (int i0 = 0; i0 < m; i0 += 32) {
+        const int i = i0 + lane;
+        const bool ok = i < m;
+        const int key = ok ? skey[i] : -1 - lane;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int rank = __popc(peers & ((1u << lane) - 1u));
+        const int start = ok ? hist[key] : 0;
+        __syncwarp();
+        if (ok) {
+          pairs[base + start + rank] = stage[i];
+          if (rank == 0) hist[key] = start + __popc(peers);
+        }
+        __syncwarp();
       }
+    } else {
+      visit(A, c, [&](bool ok, int, int sp, double, double, double, double r2) {
+        if (ok) atomicAdd(&hist[keyof(sp, r2)], 1);
+      });
       __syncwarp();
-    });
+      scan_hist();
+      visit(A, c, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double r2) {
+        const int key = ok ? keyof(sp, r2) : -1 - lane;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int rank = __popc(peers & ((1u << lane) - 1u));
+        const int start = ok ? hist[key] : 0;
+        __syncwarp();
+        if (ok) {
+          pairs[base + start + rank] =
+              make_float4((float)rx, (float)ry, (float)rz, __int_as_float(atom | (sp << kAtomBits)));
+          if (rank == 0) hist[key] = start + __popc(peers);
+        }
+        __syncwarp();
+      });
+    }
+    __syncwarp();
   }
 }
 
@@ -756,10 +806,13 @@ extern "C" int soapb_neighbors_fill(const soapb_basis* b, const soapb_structs* s
   NLWork w = nl_work(L, d_work);
   const VisitArgs A = visit_args(b, w, mode);
   if (c->n_centres > 0) {
-    const int smem = 4 * 4 * b->n_keys;
+    const int smem = 4 * (16 * kFillStage + 4 * kFillStage + 4 * b->n_keys);
+    int rc2 = check_cuda(cudaFuncSetAttribute(k_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                         "fill smem attribute");
+    if (rc2) return rc2;
     k_fill<<<grid_blocks(c->n_centres, 4), 128, smem, st>>>(A, c->n_centres, d_pair_off, (float4*)d_pairs,
-                                                            capacity, b->n_seg, 1.0 / b->seg_width, b->n_keys,
-                                                            w.status);
+                                                            capacity, b->n_seg, (float)(1.0 / b->seg_width),
+                                                            b->n_keys, w.status);
   }
   return check_launch("k_fill", c->n_centres > 0 ? 1 : 0);
 }
