@@ -21,7 +21,7 @@ W_NONE, W_W0, W_POLY, W_POW, W_EXP = range(5)
 EXPORTS = (
     "soapb_basis_plan", "soapb_basis_build", "soapb_basis_download",
     "soapb_neighbors_workspace", "soapb_neighbors_count", "soapb_neighbors_fill", "soapb_neighbors_status",
-    "soapb_neighbors_stats", "soapb_neighbors_noalloc",
+    "soapb_neighbors_stats", "soapb_neighbors_clamp", "soapb_neighbors_noalloc",
     "soapb_descriptor", "soapb_jacobian_workspace", "soapb_jacobian", "soapb_forces_workspace", "soapb_forces",
     "soapb_last_error", "soapb_version", "soapb_kernel_launches",
 )
@@ -85,6 +85,7 @@ def load() -> ctypes.CDLL:
                                  c_int64, P],
         "soapb_neighbors_status": [POINTER(Basis), POINTER(Structs), POINTER(Centres), P, POINTER(c_int32), P],
         "soapb_neighbors_stats": [POINTER(Basis), POINTER(Structs), POINTER(Centres), P, P, P, P],
+        "soapb_neighbors_clamp": [P, c_int64, c_int64, P, P],
         "soapb_neighbors_noalloc": [POINTER(Basis), POINTER(Structs), POINTER(Centres), c_int32, P, P, c_int64, P,
                                     P],
         "soapb_descriptor": [POINTER(Basis), c_int64, P, P, c_int32, P, P, P, P],

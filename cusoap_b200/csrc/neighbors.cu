@@ -651,6 +651,20 @@ __global__ void __launch_bounds__(1024) k_stats(const int64_t* pair_off, int64_t
   }
 }
 
+// One block: out[0] = the list's total; when it exceeds capacity, every
+// offset is set to 0 (all lists empty), so kernels launched after it read
+// nothing beyond the pair buffer.  One block: the total is read once before
+// any offset is rewritten.
+__global__ void __launch_bounds__(1024) k_clamp(int64_t* pair_off, int64_t n_centres, int64_t capacity, int64_t* out) {
+  __shared__ int64_t s_total;
+  if (threadIdx.x == 0) s_total = pair_off[n_centres];
+  __syncthreads();
+  const int64_t total = s_total;
+  if (threadIdx.x == 0) out[0] = total;
+  if (total <= capacity) return;
+  for (int64_t i = threadIdx.x; i <= n_centres; i += blockDim.x) pair_off[i] = 0;
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -838,6 +852,13 @@ extern "C" int soapb_neighbors_stats(const soapb_basis* b, const soapb_structs* 
   const NLWork w = nl_work(L, const_cast<void*>(d_work));
   k_stats<<<1, 1024, 0, (cudaStream_t)stream>>>(d_pair_off, c->n_centres, w.status, d_stats);
   return check_launch("k_stats");
+}
+
+extern "C" int soapb_neighbors_clamp(int64_t* d_pair_off, int64_t n_centres, int64_t capacity, int64_t* d_total,
+                                     void* stream) {
+  if (!d_pair_off || !d_total || n_centres < 0 || capacity < 0) return set_error(SOAPB_ERR_ARG, "bad clamp arguments");
+  k_clamp<<<1, 1024, 0, (cudaStream_t)stream>>>(d_pair_off, n_centres, capacity, d_total);
+  return check_launch("k_clamp");
 }
 
 // ---------------------------------------------------------------------------

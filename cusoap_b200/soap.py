@@ -228,6 +228,136 @@ class _SOAPFunction(torch.autograd.Function):
         return (-forces).to(torch.float64), None, None, None
 
 
+class SOAPBatch:
+    """A fixed batch of structures (every atom a centre) whose descriptor and
+    adjoint run as two captured CUDA graphs, for loops that re-evaluate the
+    same structures at new positions (molecular dynamics, relaxations).
+
+    Built by ``SOAP.batch(systems)``.  All buffers are allocated once: the
+    pair buffer with ``headroom`` over the first neighbour count.  Per call,
+    ``create(positions)`` copies the positions into the batch's position
+    buffer and replays the forward graph (neighbour count and fill, a clamp
+    that empties the lists if they overflowed the pair buffer, descriptor);
+    the one device-to-host read checks the pair total, and an overflow
+    rebuilds the plan with a larger buffer and replays.  The backward graph is
+    the adjoint: ``create`` is differentiable w.r.t. ``positions``.
+
+    The descriptor returned is the plan's output buffer, overwritten by the
+    next replay (clone it to keep it).  Cells, pbc, species and atom counts
+    are fixed per plan.
+    """
+
+    def __init__(self, soap: "SOAP", systems: List[Any], headroom: float = 1.25):
+        if soap.average == "cc":
+            raise NotImplementedError("SOAP.batch is built for the power spectrum (average != 'cc')")
+        self.soap = soap
+        self.headroom = float(headroom)
+        with torch.cuda.device(soap.device):
+            self.b = _Batch(soap, systems, [None] * len(systems))
+            self.counts = list(self.b.counts)
+            self.n_atoms = self.b.n_atoms
+            self._build(capacity=None)
+
+    def _build(self, capacity):
+        soap, b, lib, dev = self.soap, self.b, _lib.load(), self.soap.device
+        C = b.n_centres
+        st = _stream(dev)
+        ws = ctypes.c_int64(0)
+        check(lib.soapb_neighbors_workspace(ctypes.byref(soap._basis), ctypes.byref(b.cs), ctypes.byref(b.cc),
+                                            ctypes.byref(ws)))
+        self.work = torch.empty(max(int(ws.value), 256), dtype=torch.uint8, device=dev)
+        self.pair_off = torch.empty(C + 1, dtype=torch.int64, device=dev)
+        self.total = torch.zeros(1, dtype=torch.int64, device=dev)
+        if capacity is None:
+            check(lib.soapb_neighbors_count(ctypes.byref(soap._basis), ctypes.byref(b.cs), ctypes.byref(b.cc),
+                                            _lib.NL_ALL, _ptr(self.work), self.work.numel(), _ptr(self.pair_off), st))
+            capacity = int(int(self.pair_off[-1].item()) * self.headroom) + 1024
+        self.capacity = int(capacity)
+        self.pairs = torch.empty((self.capacity, 4), dtype=torch.float32, device=dev)
+        F, FC = int(soap._basis.n_feat_ps), int(soap._basis.n_feat_cc)
+        self.desc = torch.empty((C, F), dtype=torch.float32, device=dev)
+        self.coeff = torch.empty((C, FC), dtype=torch.float32, device=dev)
+        self.dEdp = torch.empty((C, F), dtype=torch.float32, device=dev)
+        self.forces = torch.empty((b.n_atoms, 3), dtype=torch.float32, device=dev)
+        wsb = ctypes.c_int64(0)
+        check(lib.soapb_forces_workspace(ctypes.byref(soap._basis), C, ctypes.byref(wsb)))
+        self.fwork = torch.empty(max(int(wsb.value), 256), dtype=torch.uint8, device=dev)
+        self.counter = torch.zeros(1, dtype=torch.int32, device=dev)
+        # run once eagerly (sets kernel attributes), then capture both graphs
+        self._forward_calls()
+        self._backward_calls()
+        torch.cuda.synchronize(dev)
+        self.g_fwd, self.g_bwd = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.g_fwd):
+            self._forward_calls()
+        with torch.cuda.graph(self.g_bwd):
+            self._backward_calls()
+        torch.cuda.synchronize(dev)
+
+    def _forward_calls(self):
+        soap, b, lib = self.soap, self.b, _lib.load()
+        st = _stream(soap.device)
+        bb, cs, cc = ctypes.byref(soap._basis), ctypes.byref(b.cs), ctypes.byref(b.cc)
+        check(lib.soapb_neighbors_count(bb, cs, cc, _lib.NL_ALL, _ptr(self.work), self.work.numel(),
+                                        _ptr(self.pair_off), st))
+        check(lib.soapb_neighbors_fill(bb, cs, cc, _lib.NL_ALL, _ptr(self.work), self.work.numel(),
+                                       _ptr(self.pair_off), _ptr(self.pairs), self.capacity, st))
+        check(lib.soapb_neighbors_clamp(_ptr(self.pair_off), b.n_centres, self.capacity, _ptr(self.total), st))
+        check(lib.soapb_descriptor(bb, b.n_centres, _ptr(self.pair_off), _ptr(self.pairs), _lib.OUT_PS,
+                                   _ptr(self.desc), _ptr(self.coeff), _ptr(self.counter), st))
+
+    def _backward_calls(self):
+        soap, b, lib = self.soap, self.b, _lib.load()
+        self.forces.zero_()
+        check(lib.soapb_forces(ctypes.byref(soap._basis), b.n_centres, _ptr(self.pair_off), _ptr(self.pairs),
+                               _ptr(self.coeff), _ptr(self.dEdp), _ptr(b.centre_attach), 1, _ptr(self.forces),
+                               _ptr(self.fwork), self.fwork.numel(), _ptr(self.counter), _stream(soap.device)))
+
+    def _replay_forward(self, positions: Optional[torch.Tensor]):
+        if positions is not None:
+            self.b.positions.copy_(positions.detach().reshape(-1, 3))
+        self.g_fwd.replay()
+        need = int(self.total.item())
+        if need > self.capacity:  # the lists outgrew the pair buffer: re-plan and run again
+            self._build(capacity=int(need * self.headroom) + 1024)
+            self.g_fwd.replay()
+        return self.desc
+
+    def create(self, positions: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """(n_atoms, F) descriptors of the whole batch at ``positions``
+        ((n_atoms, 3), the structures' atoms concatenated; None: unchanged).
+        Differentiable w.r.t. ``positions`` through the adjoint graph."""
+        with torch.cuda.device(self.soap.device):
+            if positions is not None and torch.is_grad_enabled() and positions.requires_grad:
+                return _BatchFunction.apply(positions, self)
+            return self._replay_forward(positions)
+
+    def forces_from(self, dEdp: torch.Tensor) -> torch.Tensor:
+        """-dE/dx (n_atoms, 3) for a given dE/dp (n_atoms, F), at the
+        positions of the last ``create``."""
+        with torch.cuda.device(self.soap.device):
+            self.dEdp.copy_(dEdp)
+            self.g_bwd.replay()
+            return self.forces
+
+    def split(self, out: torch.Tensor) -> List[torch.Tensor]:
+        """Per-structure views of a batch output."""
+        return list(torch.split(out, self.counts))
+
+
+class _BatchFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, positions, plan):
+        ctx.plan = plan
+        ctx.dtype = positions.dtype
+        return plan._replay_forward(positions)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        forces = ctx.plan.forces_from(grad_out.contiguous().to(torch.float32))
+        return (-forces).to(ctx.dtype), None
+
+
 class SOAP:
     """DScribe-compatible SOAP on B200 (see the module docstring)."""
 
@@ -545,6 +675,11 @@ class SOAP:
             pairs = _Pairs(self, batch, _lib.NL_CREATE)
             out, _ = self._run_descriptor(batch, pairs, mode)
         return out.to(self.dtype) if self.dtype != torch.float32 else out
+
+    def batch(self, systems: List[Any], headroom: float = 1.25) -> SOAPBatch:
+        """A CUDA-graph plan for repeated evaluation of the same structures
+        (every atom a centre) at new positions; see ``SOAPBatch``."""
+        return SOAPBatch(self, list(systems), headroom)
 
     def derivatives(self, system, centers=None, include=None, exclude=None, method: str = "auto",
                     return_descriptor: bool = True, attach: bool = False, n_jobs: int = 1,

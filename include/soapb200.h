@@ -171,6 +171,16 @@ int soapb_neighbors_status(const soapb_basis* b, const soapb_structs* s, const s
 int soapb_neighbors_stats(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c, const void* d_work,
                           const int64_t* d_pair_off, int64_t* d_stats, void* stream);
 
+/* For a pair buffer of fixed capacity (a captured CUDA graph replays with
+ * the buffers it was captured with): after soapb_neighbors_fill, write the
+ * list's total to *d_total (device int64) and, if it exceeds `capacity`,
+ * set every offset of d_pair_off to 0 so that the descriptor / Jacobian /
+ * adjoint kernels launched after it see empty lists instead of reading past
+ * the buffer.  The caller compares *d_total with its capacity and rebuilds
+ * with a larger buffer.  Stream-ordered, no sync.  No counterpart in the
+ * reference (it allocates per call, SG:1128-1181). */
+int soapb_neighbors_clamp(int64_t* d_pair_off, int64_t n_centres, int64_t capacity, int64_t* d_total, void* stream);
+
 /* Neighbour list that allocates nothing, for callers that cannot allocate
  * device memory when they need a list (a C/Fortran MD driver with a fixed
  * device-memory budget, or a time-step loop where cudaMalloc/cudaFree would
