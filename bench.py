@@ -207,6 +207,7 @@ def batched_vs_plain(soap_cls, torch):
     from cusoap_b200 import workloads as W
     cells = W.make("cells512")
     soap = soap_cls(**W.CONFIGS["cells512"])
+    tuned = soap.autotune(cells[:64], reps=2)  # launch shapes for (n_max 8, l_max 6, 4 species); all legs use them
     rng = np.random.default_rng(0)
     w = torch.tensor(rng.standard_normal(soap.get_number_of_features()), dtype=torch.float32, device="cuda")
     dev_cells = [{"positions": torch.tensor(c["positions"], device="cuda"), "atomic_numbers": c["atomic_numbers"],
@@ -255,7 +256,8 @@ def batched_vs_plain(soap_cls, torch):
             "batched_atoms_per_s": res["batched"], "plain_atoms_per_s": res["plain"],
             "speedup": res["batched"] / res["plain"],
             "graph_atoms_per_s": res["graph"], "graph_speedup": res["graph"] / res["plain"],
-            "graph_note": "SOAP.batch plan: forward and adjoint replayed as two captured CUDA graphs"}
+            "graph_note": "SOAP.batch plan: forward and adjoint replayed as two captured CUDA graphs",
+            "autotuned": {k: tuned[k] for k in ("desc_wpb", "desc_gn", "force_wpb")}}
 
 
 def run_batched_only(args):

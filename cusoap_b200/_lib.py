@@ -33,7 +33,7 @@ class Basis(ctypes.Structure):
         ("r_cut", c_double), ("sigma", c_double),
         ("rbf", c_int32), ("weighting", c_int32),
         ("w_r0", c_double), ("w_c", c_double), ("w_d", c_double), ("w_m", c_double), ("w_w0", c_double),
-        ("quad_n", c_int32), ("seg_hint", c_int32), ("h_poly", c_void_p),
+        ("quad_n", c_int32), ("seg_hint", c_int32), ("tune", c_int32 * 4), ("h_poly", c_void_p),
         ("eta", c_double), ("cutoff", c_double), ("seg_width", c_double),
         ("n_seg", c_int32), ("n_keys", c_int32), ("n_feat_ps", c_int32), ("n_feat_cc", c_int32),
         ("bytes", c_int64),

@@ -251,10 +251,11 @@ inline int desc_group(int N, int L) {
 }
 
 template <int L, int GN>
-static int launch_descriptor(const DescArgs& a, cudaStream_t st) {
+static int launch_descriptor(const DescArgs& a, int wpb_tuned, cudaStream_t st) {
   const int per_warp = 4 * DescShape<L>::warp_floats(a.S, a.N);
   int wpb = (200 * 1024) / per_warp;
   wpb = wpb > 4 ? 4 : wpb;
+  if ((wpb_tuned == 1 || wpb_tuned == 2 || wpb_tuned == 4) && wpb_tuned <= wpb) wpb = wpb_tuned;
   if (wpb < 1) return set_error(SOAPB_ERR_UNSUPPORTED, "descriptor shared memory %d B per warp too large", per_warp);
   const int smem = wpb * per_warp;
   auto kern = k_descriptor<L, GN>;
@@ -276,13 +277,13 @@ static int launch_descriptor(const DescArgs& a, cudaStream_t st) {
 
 template <int L>
 struct DescDispatch {
-  static int run(const DescArgs& a, int gn, cudaStream_t st) {
+  static int run(const DescArgs& a, int gn, int wpb, cudaStream_t st) {
     switch (gn) {
-      case 1: return launch_descriptor<L, 1>(a, st);
-      case 2: return launch_descriptor<L, 2>(a, st);
-      case 3: return launch_descriptor<L, 3>(a, st);
-      case 4: return launch_descriptor<L, 4>(a, st);
-      case 6: return launch_descriptor<L, 6>(a, st);
+      case 1: return launch_descriptor<L, 1>(a, wpb, st);
+      case 2: return launch_descriptor<L, 2>(a, wpb, st);
+      case 3: return launch_descriptor<L, 3>(a, wpb, st);
+      case 4: return launch_descriptor<L, 4>(a, wpb, st);
+      case 6: return launch_descriptor<L, 6>(a, wpb, st);
       default: return set_error(SOAPB_ERR_UNSUPPORTED, "descriptor: %d radial functions per lane not built", gn);
     }
   }
@@ -321,5 +322,8 @@ extern "C" int soapb_descriptor(const soapb_basis* b, int64_t n_centres, const i
   a.inv_h = (float)(1.0 / b->seg_width);
   int rc = check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st), "reset work counter");
   if (rc) return rc;
-  return dispatch_l<DescDispatch>(L, a, desc_group(N, L), st);
+  int gn = desc_group(N, L);
+  const int tg = b->tune[1];
+  if (tg > gn && (tg == 2 || tg == 3 || tg == 4 || tg == 6)) gn = tg;
+  return dispatch_l<DescDispatch>(L, a, gn, b->tune[0], st);
 }

@@ -318,7 +318,7 @@ static int resident_blocks(const void* kern, int threads, int smem, int* out) {
 
 template <int L>
 struct ForceDispatch {
-  static int run(const ForceArgs& a, cudaStream_t st) {
+  static int run(const ForceArgs& a, int wpb_tuned, cudaStream_t st) {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -355,7 +355,7 @@ struct ForceDispatch {
     // edges
     auto kern = k_forces<L>;
     const int per_warp = 4 * ForceShape<L>::warp_floats(a.S, a.N);
-    int wpb = 4;
+    int wpb = (wpb_tuned == 1 || wpb_tuned == 2 || wpb_tuned == 4) ? wpb_tuned : 4;
     while (wpb > 1 && wpb * per_warp > 200 * 1024) wpb >>= 1;
     if (wpb * per_warp > 200 * 1024)
       return set_error(SOAPB_ERR_UNSUPPORTED, "forces: %d B of shared memory per warp is too large", per_warp);
@@ -426,5 +426,5 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.inv_h = (float)(1.0 / b->seg_width);
   int rc = check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st), "reset work counter");
   if (rc) return rc;
-  return dispatch_l<ForceDispatch>(b->l_max, a, st);
+  return dispatch_l<ForceDispatch>(b->l_max, a, b->tune[2], st);
 }

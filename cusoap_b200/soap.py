@@ -676,6 +676,13 @@ class SOAP:
             out, _ = self._run_descriptor(batch, pairs, mode)
         return out.to(self.dtype) if self.dtype != torch.float32 else out
 
+    def autotune(self, system, reps: int = 3, cache_path: Optional[str] = None, force: bool = False):
+        """Time the candidate launch shapes of the descriptor and adjoint
+        kernels on ``system`` and keep the fastest for this object (see
+        ``cusoap_b200.autotune``); results are bitwise unchanged."""
+        from .autotune import autotune
+        return autotune(self, system, reps=reps, cache_path=cache_path, force=force)
+
     def batch(self, systems: List[Any], headroom: float = 1.25) -> SOAPBatch:
         """A CUDA-graph plan for repeated evaluation of the same structures
         (every atom a centre) at new positions; see ``SOAPBatch``."""
