@@ -299,13 +299,14 @@ def run_batched_only(args):
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA at the 1965 MHz max clock
 
 
-def scale_create(soap_cls, torch, steps: int = 3, warmup: int = 2):
+def scale_create(soap_cls, torch, steps: int = 3, warmup: int = 2, n_mol: int = 0):
     """The scale workload: create() on the 1,000,002-atom water cluster
     (n_max 8, l_max 4, F = 680, 2.72 GB of output), positions resident on the
     device.  Reports atoms/s and the descriptor kernel against both its HBM
-    traffic (pairs read + rows written) and its FP32 work."""
+    traffic (pairs read + rows written) and its FP32 work.  n_mol > 0: the
+    same lattice cut to n_mol molecules (a smaller profiling case)."""
     from cusoap_b200 import workloads as W
-    sysd = W.make("cluster1M")
+    sysd = W.make("cluster1M") if n_mol <= 0 else W.water_cluster(70, 70, 69, n_mol=n_mol, seed=0)
     soap = soap_cls(**W.CONFIGS["cluster1M"])
     pos = torch.tensor(sysd["positions"], dtype=torch.float64, device="cuda")
     system = {"positions": pos, "atomic_numbers": sysd["atomic_numbers"]}
@@ -334,8 +335,8 @@ def scale_create(soap_cls, torch, steps: int = 3, warmup: int = 2):
     byts = n_pairs * 16 + n_at * F * 4
     d_ms = st.get("descriptor", float("nan"))
     peak, _ = _peaks()
-    return {"workload": "(H2O)_333334 non-periodic cluster, 1,000,002 atoms; r_cut 6, n_max 8, l_max 4, sigma 1; "
-                        "create() only, positions on the device",
+    return {"workload": f"(H2O)_{n_at // 3} non-periodic cluster, {n_at:,} atoms; r_cut 6, n_max 8, l_max 4, "
+                        "sigma 1; create() only, positions on the device",
             "atoms_per_s": n_at * steps / (e0.elapsed_time(e1) / 1e3), "ms_per_step": e0.elapsed_time(e1) / steps,
             "stage_ms_per_step": st, "pairs": n_pairs,
             "descriptor": {"hbm_bytes": byts, "gbs": byts / d_ms / 1e6, "hbm_frac_of_measured": byts / d_ms / 1e6 / peak,
@@ -498,12 +499,15 @@ def main():
                     help="profiling case: run only the batched path on the first K cells")
     ap.add_argument("--scale-only", action="store_true",
                     help="profiling case: run only the 1,000,002-atom create() leg and print its object")
+    ap.add_argument("--scale-mol", type=int, default=0,
+                    help="with --scale-only: cut the cluster to this many molecules (smaller profiling case)")
     args = ap.parse_args()
     if args.scale_only:
         import torch
         from cusoap_b200 import SOAP
         torch.cuda.set_device(0)
-        print(json.dumps(scale_create(SOAP, torch, steps=args.steps, warmup=args.warmup)), flush=True)
+        print(json.dumps(scale_create(SOAP, torch, steps=args.steps, warmup=args.warmup, n_mol=args.scale_mol)),
+              flush=True)
     elif args.batched_cells > 0:
         run_batched_only(args)
     elif args.impl == "reference":

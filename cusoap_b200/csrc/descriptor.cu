@@ -173,14 +173,15 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
         float B[GN];
 #pragma unroll
         for (int g = 0; g < GN; ++g) B[g] = (t > 2.0f) ? selfb[g] : horner7(cf[g], t);
+        // all M slots, without a per-lane test: slots m >= 2l+1 read the next
+        // harmonics of the row (index <= l^2 + 2L < K, in bounds) and collect
+        // values that flush() never stores, so no branch is needed per slot
         const float* yr = Y + q * YS + lme * lme;
 #pragma unroll
         for (int m = 0; m < M; ++m) {
-          if (m < mme) {
-            const float yv = yr[m];
+          const float yv = yr[m];
 #pragma unroll
-            for (int g = 0; g < GN; ++g) acc[g][m] = fmaf(B[g], yv, acc[g][m]);
-          }
+          for (int g = 0; g < GN; ++g) acc[g][m] = fmaf(B[g], yv, acc[g][m]);
         }
       }
       __syncwarp();

@@ -42,8 +42,7 @@ struct NLWork {
   int* bin_cursor;           // (max_bins)
   int* atom_bin;             // (n_atoms)
   int* sorted_atom;          // (n_atoms)
-  double4* sorted_pos;       // (n_atoms) wrapped positions
-  int4* sorted_info;         // (n_atoms) {atom, species, wrap, 0}
+  double4* sorted_pos;       // (n_atoms) {wrapped x, y, z, packed info} (see pack_info)
   double4* cpos;             // (n_centres) wrapped centre positions
   int4* cinfo;               // (n_centres) {bin xyz, struct, wrap, atom}
   int* counts;               // (n_centres)
@@ -76,6 +75,20 @@ __device__ __forceinline__ void unpack3(int p, int (&v)[3]) {
   v[0] = (p & 1023) - 512;
   v[1] = ((p >> 10) & 1023) - 512;
   v[2] = ((p >> 20) & 1023) - 512;
+}
+// atom (27 bits) | species (5 bits) | packed wrap shifts (30 bits), carried in
+// the fourth double of a sorted-atom record so a candidate is one 32-byte load
+// (the bits are only moved, never used as a floating-point value).
+__device__ __forceinline__ double pack_info(int atom, int sp, int wrap) {
+  const unsigned long long bits = (unsigned long long)(unsigned)atom | ((unsigned long long)(unsigned)sp << kAtomBits) |
+                                  ((unsigned long long)(unsigned)wrap << 32);
+  return __longlong_as_double((long long)bits);
+}
+__device__ __forceinline__ void unpack_info(double w, int& atom, int& sp, int& wrap) {
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(w);
+  atom = (int)(bits & kAtomMask);
+  sp = (int)((bits >> kAtomBits) & 31u);
+  wrap = (int)(bits >> 32);
 }
 __device__ __forceinline__ int floordiv(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
 
@@ -415,8 +428,7 @@ __global__ void k_gather_atoms(soapb_structs s, NLWork w) {
     double wp[3];
     locate(g, s.d_positions[3 * (int64_t)a], s.d_positions[3 * (int64_t)a + 1], s.d_positions[3 * (int64_t)a + 2],
            b, wr, wp);
-    w.sorted_pos[slot] = make_double4(wp[0], wp[1], wp[2], 0.0);
-    w.sorted_info[slot] = make_int4(a, s.d_species[a], pack3(wr[0], wr[1], wr[2]), 0);
+    w.sorted_pos[slot] = make_double4(wp[0], wp[1], wp[2], pack_info((int)a, s.d_species[a], pack3(wr[0], wr[1], wr[2])));
   }
 }
 
@@ -442,7 +454,6 @@ struct VisitArgs {
   const int64_t* bin_off;
   const int64_t* bin_start;
   const double4* sorted_pos;
-  const int4* sorted_info;
   const double4* cpos;
   const int4* cinfo;
   double cutoff2;
@@ -484,7 +495,8 @@ __device__ __forceinline__ void visit(const VisitArgs& A, int64_t c, Fn&& fn) {
           double rx = 0.0, ry = 0.0, rz = 0.0, r2 = 0.0;
           if (i < s1) {
             const double4 p = A.sorted_pos[i];
-            const int4 inf = A.sorted_info[i];
+            int wrap;
+            unpack_info(p.w, atom, sp, wrap);
             rx = p.x + sx;
             ry = p.y + sy;
             rz = p.z + sz;
@@ -492,15 +504,13 @@ __device__ __forceinline__ void visit(const VisitArgs& A, int64_t c, Fn&& fn) {
             ok = r2 <= A.cutoff2;
             if (ok && g.any_per) {
               int aw[3];
-              unpack3(inf.z, aw);
+              unpack3(wrap, aw);
 #pragma unroll
               for (int k = 0; k < 3; ++k)
                 if (g.per[k]) ok &= abs(T[k] - aw[k] + cw[k]) <= g.nrep[k];
             }
             // create(): drop r <= 1e-12 edges except the centre's own atom (SG:1171-1179)
-            if (ok && A.mode == SOAPB_NL_CREATE && r2 <= 1e-24 && inf.x != ci.w) ok = false;
-            atom = inf.x;
-            sp = inf.y;
+            if (ok && A.mode == SOAPB_NL_CREATE && r2 <= 1e-24 && atom != ci.w) ok = false;
           }
           fn(ok, atom, sp, rx, ry, rz, r2);
         }
@@ -670,8 +680,8 @@ __global__ void __launch_bounds__(1024) k_clamp(int64_t* pair_off, int64_t n_cen
 // ---------------------------------------------------------------------------
 
 struct NLLayout {
-  int64_t grids, fbox, bps, bin_off, bin_count, bin_start, bin_cursor, atom_bin, sorted_atom, sorted_pos,
-      sorted_info, cpos, cinfo, counts, partials, status, total;
+  int64_t grids, fbox, bps, bin_off, bin_count, bin_start, bin_cursor, atom_bin, sorted_atom, sorted_pos, cpos,
+      cinfo, counts, partials, status, total;
   int64_t max_bins;
 };
 
@@ -692,7 +702,6 @@ static NLLayout nl_layout(const soapb_structs* s, const soapb_centres* c) {
   L.atom_bin = take(4 * na);
   L.sorted_atom = take(4 * na);
   L.sorted_pos = take(32 * na);
-  L.sorted_info = take(16 * na);
   L.cpos = take(32 * nc);
   L.cinfo = take(16 * nc);
   L.counts = take(4 * nc);
@@ -715,7 +724,6 @@ static NLWork nl_work(const NLLayout& L, void* base_) {
   w.atom_bin = (int*)(base + L.atom_bin);
   w.sorted_atom = (int*)(base + L.sorted_atom);
   w.sorted_pos = (double4*)(base + L.sorted_pos);
-  w.sorted_info = (int4*)(base + L.sorted_info);
   w.cpos = (double4*)(base + L.cpos);
   w.cinfo = (int4*)(base + L.cinfo);
   w.counts = (int*)(base + L.counts);
@@ -743,7 +751,6 @@ static VisitArgs visit_args(const soapb_basis* b, const NLWork& w, int mode) {
   A.bin_off = w.bin_off;
   A.bin_start = w.bin_start;
   A.sorted_pos = w.sorted_pos;
-  A.sorted_info = w.sorted_info;
   A.cpos = w.cpos;
   A.cinfo = w.cinfo;
   A.cutoff2 = b->cutoff * b->cutoff;
@@ -910,7 +917,7 @@ extern "C" int soapb_neighbors_noalloc(const soapb_basis* b, const soapb_structs
   if (L.total > kNoAllocScratchBytes)
     return set_error(SOAPB_ERR_ARG,
                      "soapb_neighbors_noalloc: this input needs %lld bytes of scratch but the fixed scratch array "
-                     "holds %lld bytes (about 55,000 atoms with every atom a centre); use soapb_neighbors_count/_fill with a workspace",
+                     "holds %lld bytes (about 67,000 atoms with every atom a centre); use soapb_neighbors_count/_fill with a workspace",
                      (long long)L.total, (long long)kNoAllocScratchBytes);
   void* scratch = nullptr;
   if ((rc = scratch_address(&scratch))) return rc;

@@ -192,7 +192,7 @@ int soapb_neighbors_clamp(int64_t* d_pair_off, int64_t n_centres, int64_t capaci
  * inputs and outputs as soapb_neighbors_count + soapb_neighbors_fill, but
  * the workspace is a fixed 8 MiB device array inside the library (held on
  * every GPU that loads it until the process exits), enough for about
- * 55,000 atoms when every atom is a centre (~140 bytes per atom); larger inputs return SOAPB_ERR_ARG before
+ * 67,000 atoms when every atom is a centre (~124 bytes per atom); larger inputs return SOAPB_ERR_ARG before
  * anything is launched.  Pairs are written only when the total
  * d_pair_off[n_centres] fits `capacity`; *d_status (device int32) receives
  * the error flags of soapb_neighbors_status (bit 2 = capacity too small).
