@@ -151,17 +151,22 @@ __device__ __forceinline__ void bulk_s2g(void* g, const void* s, uint32_t bytes)
                : "memory");
 }
 
-// Zero rows of chunks blockIdx, blockIdx + gridDim, ... (64 rows each, global
-// row order) by TMA bulk copies of the zero tile; lane 0 issues, the copies run
+// Zero rows of 64-row chunks (global row order) claimed from a work queue
+// (zq), by TMA bulk copies of the zero tile; lane 0 issues, the copies run
 // asynchronously and the lane waits for all of them before returning (the
-// tile must outlive them).  Rows are 12 F bytes, a multiple of 16 (F % 4 == 0).
-__device__ void jac_zero_rows_tma(const JacArgs& a, const void* ztile) {
+// tile must outlive them).  Every block's zero warp runs this from the start
+// and its compute warps join once the centre queue is empty, so the zero
+// stream ends together with the compute work.  Rows are 12 F bytes, a
+// multiple of 16 (F % 4 == 0).
+__device__ void jac_zero_rows_tma(const JacArgs& a, const void* ztile, int* zq) {
   if ((threadIdx.x & 31) != 0) return;
   const int64_t nrows = a.n_centres * a.n_inc;
   const int64_t row_bytes = 12 * (int64_t)a.F;
   const int64_t nchunks = (nrows + kZeroChunkRows - 1) / kZeroChunkRows;
   char* out = reinterpret_cast<char*>(a.out);
-  for (int64_t k = blockIdx.x; k < nchunks; k += gridDim.x) {
+  for (;;) {
+    const int64_t k = (int64_t)(unsigned)atomicAdd(zq, 1);
+    if (k >= nchunks) break;
     const int64_t r0 = k * kZeroChunkRows, r1 = min(r0 + (int64_t)kZeroChunkRows, nrows);
     int64_t run = -1;
     for (int64_t r = r0; r <= r1; ++r) {
@@ -374,7 +379,7 @@ __global__ void __launch_bounds__(256) k_jacobian(JacArgs a) {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // tile visible to the bulk-copy engine
   __syncthreads();
   if (threadIdx.x < 32) {  // zero role
-    if (vec) jac_zero_rows_tma(a, ztile);
+    if (vec) jac_zero_rows_tma(a, ztile, a.counter + 1);
     else jac_zero_rows_st(a);
     return;
   }
@@ -441,6 +446,8 @@ __global__ void __launch_bounds__(256) k_jacobian(JacArgs a) {
       compute_bar(kCT);  // staged entries are rewritten by the next batch
     }
   }
+  // centre queue empty: this warp joins the zero-row stream
+  if (vec) jac_zero_rows_tma(a, ztile, a.counter + 1);
 }
 
 // ---------------------------------------------------------------------------
