@@ -312,9 +312,12 @@ __global__ void k_grid_setup(soapb_structs s, NLWork w, double cutoff) {
     perp[k] = det / (sqrt(cx * cx + cy * cy + cz * cz) + 1e-300);
   }
   const int64_t A = s.d_atom_off[i + 1] - s.d_atom_off[i];
+  // bins of perpendicular width >= cutoff / 2 (a +-2 bin window): 5^3 half-width
+  // bins hold 15.6 cutoff^3 of candidates against 27 cutoff^3 for full-width bins
+  const double bin_min = 0.5 * cutoff;
   for (int k = 0; k < 3; ++k) {
     if (g.per[k]) {
-      const int nb = (int)floor(perp[k] / cutoff);
+      const int nb = (int)floor(perp[k] / bin_min);
       g.nb[k] = min(max(nb, 1), 1023);
       g.fmin[k] = 0.0;
       g.binw[k] = 1.0 / g.nb[k];
@@ -322,7 +325,7 @@ __global__ void k_grid_setup(soapb_structs s, NLWork w, double cutoff) {
       double lo = ord_decode(w.fbox[i * 6 + k]), hi = ord_decode(w.fbox[i * 6 + 3 + k]);
       if (!(hi >= lo)) { lo = 0.0; hi = 0.0; }  // no atoms
       const double span = hi - lo;
-      const int nb = (int)floor(span * perp[k] / cutoff);
+      const int nb = (int)floor(span * perp[k] / bin_min);
       g.nb[k] = min(max(nb, 1), 1023);
       g.fmin[k] = lo;
       g.binw[k] = span > 0.0 ? span / g.nb[k] : 1.0;
@@ -478,16 +481,28 @@ __device__ __forceinline__ void visit(const VisitArgs& A, int64_t c, Fn&& fn) {
       int by = cb[1] + dy, Ty = 0;
       if (g.per[1]) { Ty = floordiv(by, g.nb[1]); by -= Ty * g.nb[1]; }
       else if (by < 0 || by >= g.nb[1]) continue;
-      for (int dx = -g.win[0]; dx <= g.win[0]; ++dx) {
-        int bx = cb[0] + dx, Tx = 0;
-        if (g.per[0]) { Tx = floordiv(bx, g.nb[0]); bx -= Tx * g.nb[0]; }
-        else if (bx < 0 || bx >= g.nb[0]) continue;
+      // the row's x bins as runs of consecutive bins with one image shift Tx:
+      // a run is one contiguous range of bin-sorted atoms
+      int dx = -g.win[0];
+      while (dx <= g.win[0]) {
+        int bx = cb[0] + dx, Tx = 0, run_end;
+        if (g.per[0]) {
+          Tx = floordiv(bx, g.nb[0]);
+          bx -= Tx * g.nb[0];
+          run_end = min(g.win[0], dx + (g.nb[0] - 1 - bx));
+        } else {
+          if (bx < 0) { dx = -cb[0]; continue; }
+          if (bx >= g.nb[0]) break;
+          run_end = min(g.win[0], g.nb[0] - 1 - cb[0]);
+        }
+        const int bx1 = bx + (run_end - dx);
+        dx = run_end + 1;
         const double sx = Tx * g.H[0] + Ty * g.H[3] + Tz * g.H[6] - cp.x;
         const double sy = Tx * g.H[1] + Ty * g.H[4] + Tz * g.H[7] - cp.y;
         const double sz = Tx * g.H[2] + Ty * g.H[5] + Tz * g.H[8] - cp.z;
         const int T[3] = {Tx, Ty, Tz};
-        const int64_t gb = boff + ((int64_t)bz * g.nb[1] + by) * g.nb[0] + bx;
-        const int64_t s0 = A.bin_start[gb], s1 = A.bin_start[gb + 1];
+        const int64_t gb = boff + ((int64_t)bz * g.nb[1] + by) * g.nb[0];
+        const int64_t s0 = A.bin_start[gb + bx], s1 = A.bin_start[gb + bx1 + 1];
         for (int64_t base = s0; base < s1; base += 32) {
           const int64_t i = base + lane;
           bool ok = false;

@@ -713,9 +713,12 @@ class SOAP:
             desc, coeff = self._run_descriptor(batch, pairs, mode, want_coeff=True)
             deriv = torch.empty((batch.n_centres, n_inc, 3, F), dtype=torch.float32, device=self.device)
             if n_inc > 0 and batch.n_centres > 0:
-                inc_row = torch.full((max(n_atoms, 1),), -1, dtype=torch.int32)
-                inc_row[torch.tensor(idx, dtype=torch.int64)] = torch.arange(n_inc, dtype=torch.int32)
-                inc_row = inc_row.to(self.device)
+                if include is None and exclude is None:  # every atom, in order: row = atom
+                    inc_row = torch.arange(max(n_atoms, 1), dtype=torch.int32, device=self.device)
+                else:
+                    h = np.full(max(n_atoms, 1), -1, dtype=np.int32)
+                    h[np.asarray(idx, dtype=np.int64)] = np.arange(n_inc, dtype=np.int32)
+                    inc_row = torch.from_numpy(h).to(self.device)
                 status = torch.zeros(1, dtype=torch.int32, device=self.device)
                 lib = _lib.load()
                 wsb = ctypes.c_int64(0)
