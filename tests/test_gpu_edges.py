@@ -1,0 +1,74 @@
+"""Edge cases on the GPU against the FP64 oracle: empty centre lists and
+empty structures inside a batch (ragged batches), the largest l_max the
+library is built for (l_max 9, with n_max 10: the widest kernel
+instantiations), and Cartesian centres on and off atoms."""
+import numpy as np
+import pytest
+import torch
+
+from oracle.soap_oracle import OracleSOAP, rel_l2
+from cusoap_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+DESC_TOL = 1e-5
+DERIV_TOL = 1e-4
+
+
+def _row_err(a, b):
+    a = np.asarray(a, np.float64).reshape(a.shape[0], -1)
+    b = np.asarray(b, np.float64).reshape(b.shape[0], -1)
+    nb = np.linalg.norm(b, axis=1)
+    return float(np.max(np.linalg.norm(a - b, axis=1) / np.where(nb > 0, nb, 1.0)))
+
+
+def test_empty_centres_and_empty_structure_in_a_batch():
+    from cusoap_b200 import SOAP
+    P = dict(W.CONFIGS["cluster192"])
+    s = SOAP(**P)
+    o = OracleSOAP(**P)
+    sysd = W.water_cluster(2, 2, 2, seed=1)
+    out = s.create(sysd, centers=[])
+    assert tuple(out.shape) == (0, s.get_number_of_features())
+    empty = {"positions": np.zeros((0, 3)), "atomic_numbers": np.zeros(0, dtype=np.int64)}
+    one = {"positions": np.zeros((1, 3)), "atomic_numbers": np.array([8])}
+    outs = s.create([sysd, empty, one, sysd])
+    assert isinstance(outs, list) and [int(x.shape[0]) for x in outs] == [24, 0, 1, 24]
+    ref = o.create(sysd["positions"], sysd["atomic_numbers"])
+    assert _row_err(outs[0].cpu().numpy(), ref) < DESC_TOL
+    assert torch.equal(outs[0], outs[3])
+    assert _row_err(outs[2].cpu().numpy(), o.create(one["positions"], one["atomic_numbers"])) < DESC_TOL
+
+
+def test_largest_l_max_create_derivatives_forces():
+    from cusoap_b200 import SOAP
+    P = dict(species=[1, 8], r_cut=4.0, n_max=10, l_max=9, sigma=0.5)
+    s = SOAP(**P)
+    o = OracleSOAP(**P)
+    sysd = W.water_cluster(2, 2, 2, seed=6)
+    pos, Z = sysd["positions"], sysd["atomic_numbers"]
+    assert _row_err(s.create(sysd).cpu().numpy(), o.create(pos, Z)) < DESC_TOL
+    J = s.derivatives(sysd, centers=[0, 5], include=list(range(10)), return_descriptor=False)
+    Jo = o.derivatives(pos, Z, centers=[0, 5], include=list(range(10)), return_descriptor=False)
+    assert _row_err(J.cpu().numpy(), Jo) < DERIV_TOL
+    w = np.random.default_rng(0).standard_normal(s.get_number_of_features())
+    pt = torch.tensor(pos, device="cuda", requires_grad=True)
+    (s.create({"positions": pt, "atomic_numbers": Z}) * torch.tensor(w, dtype=torch.float32,
+                                                                     device="cuda")).sum().backward()
+    Fo = o.forces(pos, Z, np.tile(w, (len(Z), 1)))
+    assert rel_l2(-pt.grad.cpu().numpy(), Fo) < DERIV_TOL
+
+
+def test_cartesian_centres_on_and_off_atoms_derivatives():
+    from cusoap_b200 import SOAP
+    P = dict(W.CONFIGS["cluster192"])
+    s = SOAP(**P)
+    o = OracleSOAP(**P)
+    sysd = W.water_cluster(2, 2, 2, seed=2)
+    pos, Z = sysd["positions"], sysd["atomic_numbers"]
+    cen = [pos[3].tolist(), [0.5, 0.25, 1.0], 7]
+    d = s.create(sysd, centers=cen).cpu().numpy()
+    assert _row_err(d, o.create(pos, Z, centers=cen)) < DESC_TOL
+    J = s.derivatives(sysd, centers=cen, return_descriptor=False).cpu().numpy()
+    Jo = o.derivatives(pos, Z, centers=cen, return_descriptor=False)
+    assert _row_err(J, Jo) < DERIV_TOL
