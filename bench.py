@@ -221,7 +221,7 @@ def batched_vs_plain(soap_cls, torch):
             d["positions"] = c["positions"].clone().requires_grad_(True)
             sysl.append(d)
         out = soap.create(sysl)  # a list: the cells differ in size
-        E = ((torch.cat(out) if isinstance(out, list) else out) * w).sum()
+        E = ((torch.cat(out) if isinstance(out, list) else out) @ w).sum()
         E.backward()
         return sysl
 
@@ -229,14 +229,14 @@ def batched_vs_plain(soap_cls, torch):
         for c in dev_cells:
             d = dict(c)
             d["positions"] = c["positions"].clone().requires_grad_(True)
-            (soap.create(d) * w).sum().backward()
+            (soap.create(d) @ w).sum().backward()
 
     plan = soap.batch(cells)
     pos_all = torch.cat([c["positions"] for c in dev_cells])
 
     def graph():
         pos = pos_all.clone().requires_grad_(True)
-        (plan.create(pos) * w).sum().backward()
+        (plan.create(pos) @ w).sum().backward()
         return pos
 
     res = {}
@@ -278,7 +278,7 @@ def run_batched_only(args):
     def one():
         sysl = [dict(c, positions=c["positions"].clone().requires_grad_(True)) for c in dev_cells]
         out = soap.create(sysl)
-        E = ((torch.cat(out) if isinstance(out, list) else out) * w).sum()
+        E = ((torch.cat(out) if isinstance(out, list) else out) @ w).sum()
         E.backward()
 
     one()

@@ -126,16 +126,8 @@ class _Batch:
         self.atom_off_list = atom_off.tolist()
         self.n_atoms = int(atom_off[-1])
         self.pos_tensors = [r[0] for r in raw if isinstance(r[0], torch.Tensor)]
-        if all(isinstance(r[0], np.ndarray) for r in raw):
-            host = np.concatenate([r[0] for r in raw]) if raw else np.zeros((0, 3))
-            self.positions = torch.as_tensor(np.ascontiguousarray(host, dtype=np.float64)).to(dev)
-            self.pos_tensors = []
-        else:
-            parts = [r[0].detach().to(dev, torch.float64) if isinstance(r[0], torch.Tensor)
-                     else torch.as_tensor(r[0], dtype=torch.float64, device=dev) for r in raw]
-            self.positions = torch.cat(parts).contiguous()
+        host_pos = all(isinstance(r[0], np.ndarray) for r in raw)
         Zall = np.concatenate([r[1] for r in raw]) if raw else np.zeros(0, np.int64)
-        self.species = soap._species_index(Zall)
         cells = np.zeros((len(raw), 9))
         pbcs = np.zeros((len(raw), 3), np.uint8)
         if soap.periodic:
@@ -146,18 +138,33 @@ class _Batch:
                                       dtype=np.float64).reshape(9)
                 pbcs[i] = np.asarray(r[3].detach().cpu() if isinstance(r[3], torch.Tensor) else r[3],
                                      dtype=bool).reshape(3)
-        self.atom_off = torch.as_tensor(atom_off).to(dev)
-        self.cells = torch.as_tensor(cells).to(dev)
-        self.pbc = torch.as_tensor(pbcs).to(dev)
-        if all(c is None for c in centers_list):
+        all_atoms = all(c is None for c in centers_list)
+        # the small host arrays (and host positions) go to the device in ONE
+        # asynchronous copy from a pinned staging buffer
+        arrays = [("species", soap._species_lookup(Zall)), ("atom_off", atom_off), ("cells", cells), ("pbc", pbcs)]
+        if all_atoms:
+            arrays.append(("centre_struct", np.repeat(np.arange(len(raw), dtype=np.int32), counts_a)))
+        if host_pos:
+            host = np.concatenate([r[0] for r in raw]) if raw else np.zeros((0, 3))
+            arrays.append(("positions", np.ascontiguousarray(host, dtype=np.float64)))
+        dev_arrays = soap._upload(arrays)
+        self.species, self.atom_off = dev_arrays["species"], dev_arrays["atom_off"]
+        self.cells, self.pbc = dev_arrays["cells"], dev_arrays["pbc"]
+        if host_pos:
+            self.positions = dev_arrays["positions"]
+            self.pos_tensors = []
+        else:
+            parts = [r[0].detach().to(dev, torch.float64) if isinstance(r[0], torch.Tensor)
+                     else torch.as_tensor(r[0], dtype=torch.float64, device=dev) for r in raw]
+            self.positions = torch.cat(parts).contiguous()
+        if all_atoms:
             # every atom is a centre, attached to itself (SG:977-979)
             self.counts = counts_a
             self.n_centres = self.n_atoms
             self.centre_xyz = self.positions
             self.centre_atom = torch.arange(self.n_atoms, dtype=torch.int32, device=dev)
             self.centre_attach = self.centre_atom
-            self.centre_struct = torch.as_tensor(
-                np.repeat(np.arange(len(raw), dtype=np.int32), counts_a)).to(dev)
+            self.centre_struct = dev_arrays["centre_struct"]
         else:
             cxyz, cstruct, catom, cattach, self.counts = [], [], [], [], []
             for i, cen in enumerate(centers_list):
@@ -554,7 +561,9 @@ class SOAP:
             return as_pos(system.get_positions()), as_z(system.get_atomic_numbers()), cell, pbc
         raise TypeError("Unsupported system type. Provide ASE.Atoms-like, dict, or (positions, Z, cell, pbc).")
 
-    def _species_index(self, Z) -> torch.Tensor:
+    def _species_lookup(self, Z) -> np.ndarray:
+        """Host int32 species index of every atom; ValueError for atomic
+        numbers outside the species list (SG:1782-1784)."""
         Zc = Z.detach().cpu().numpy() if isinstance(Z, torch.Tensor) else np.asarray(Z, dtype=np.int64)
         bad = set(np.unique(Zc).tolist()) - self._atomic_number_set
         if bad:
@@ -563,7 +572,40 @@ class SOAP:
         for z, i in self._Z_to_species_index.items():
             if z < lut.size:
                 lut[z] = i
-        return torch.as_tensor(lut[Zc] if Zc.size else np.zeros(0, np.int32)).to(self.device)
+        return lut[Zc] if Zc.size else np.zeros(0, np.int32)
+
+    def _species_index(self, Z) -> torch.Tensor:
+        return torch.as_tensor(self._species_lookup(Z)).to(self.device)
+
+    def _upload(self, arrays) -> Dict[str, torch.Tensor]:
+        """Copy named host arrays to the device in one asynchronous copy
+        through a pinned staging buffer kept by this object; returns typed
+        device views.  The staging buffer is reused once its last copy has
+        completed."""
+        offs, off = [], 0
+        for name, a in arrays:
+            a = np.ascontiguousarray(a)
+            offs.append((name, a, off))
+            off = (off + a.nbytes + 255) // 256 * 256
+        total = max(off, 256)
+        if getattr(self, "_stage", None) is None or self._stage.numel() < total:
+            self._stage = torch.empty(max(total, 1 << 16), dtype=torch.uint8, pin_memory=True)
+            self._stage_done = None
+        if self._stage_done is not None:
+            self._stage_done.synchronize()
+        host = self._stage.numpy()
+        for name, a, o in offs:
+            host[o:o + a.nbytes] = a.view(np.uint8).reshape(-1)
+        dbuf = torch.empty(total, dtype=torch.uint8, device=self.device)
+        dbuf.copy_(self._stage[:total], non_blocking=True)
+        self._stage_done = torch.cuda.Event()
+        self._stage_done.record(torch.cuda.current_stream(self.device))
+        tmap = {np.dtype(np.int32): torch.int32, np.dtype(np.int64): torch.int64,
+                np.dtype(np.float64): torch.float64, np.dtype(np.uint8): torch.uint8}
+        out = {}
+        for name, a, o in offs:
+            out[name] = dbuf[o:o + a.nbytes].view(tmap[a.dtype]).reshape(a.shape)
+        return out
 
     def _prepare_centres(self, pos: torch.Tensor, centers):
         """(xyz, self atom, attached atom) per centre.  Index centres are
