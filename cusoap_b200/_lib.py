@@ -93,7 +93,7 @@ def load() -> ctypes.CDLL:
         "soapb_jacobian": [POINTER(Basis), c_int64, P, P, c_int64, P, P, c_int64, P, c_int32, c_int32, c_int32, P,
                            P, c_int64, P, P],
         "soapb_forces_workspace": [POINTER(Basis), c_int64, POINTER(c_int64)],
-        "soapb_forces": [POINTER(Basis), c_int64, P, P, P, P, P, c_int32, P, P, c_int64, P, P],
+        "soapb_forces": [POINTER(Basis), c_int64, P, P, P, P, c_int32, P, c_int32, P, P, c_int64, P, P],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
   }
   __syncthreads();
   const int nblk = a.crossover ? S * (S + 1) / 2 : S;
+  const int q32 = 32 / N, r32 = 32 % N;  // p -> p + 32 in the off-diagonal (n, n') order
 
   // lane -> l and its functions n = k GN + g
   const int l_me = lane / LPL, k_me = lane % LPL;
@@ -206,14 +207,11 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
 #pragma unroll
         for (int l = 0; l <= L; ++l) {
           float* o = orow + fb0 + l * np;
+          int n = lane / N, nd = lane - (lane / N) * N;  // off-diagonal (n, n') of p, advanced by 32 per step
           for (int p = lane; p < np; p += 32) {
-            int n, nd;
             if (diag) {
               n = s_tri[2 * p];
               nd = s_tri[2 * p + 1];
-            } else {
-              n = p / N;
-              nd = p - n * N;
             }
             const float* x = cbuf + (j * N + n) * KC + l * l;
             const float* y = cbuf + (jd * N + nd) * KC + l * l;
@@ -221,6 +219,11 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
 #pragma unroll
             for (int m = 0; m < 2 * l + 1; ++m) s = fmaf(x[m], y[m], s);
             o[p] = s * s_pref[l];
+            if (!diag) {
+              n += q32;
+              nd += r32;
+              if (nd >= N) { nd -= N; ++n; }
+            }
           }
         }
       }

@@ -167,6 +167,21 @@ __global__ void __launch_bounds__(kGThreads) k_adjoint_g_dense(ForceArgs a) {
   }
 }
 
+// G = dE/dc for the cc output (E = sum dEdp . cc-projection): the cc layout's
+// l = 1 permutation and pi^-3/2 scale (lm >= 4) run backwards, elementwise.
+__global__ void k_adjoint_g_cc(ForceArgs a, int K) {
+  const int64_t SNK = (int64_t)a.S * a.N * K;
+  const float pi_m15 = (float)(1.0 / (kPi * 1.7724538509055160273));
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n_centres * SNK;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = i / SNK, r = i - c * SNK;
+    const int lm = (int)(r % K);
+    // output position of source lm: l = 1 is stored (z, x, y) = source (2, 3, 1)
+    const int dst = (lm == 1) ? 3 : (lm == 2) ? 1 : (lm == 3) ? 2 : lm;
+    a.G[i] = a.dEdp[c * SNK + (r - lm) + dst] * (lm >= 4 ? pi_m15 : 1.0f);
+  }
+}
+
 // Q_l^m table and the powers (x + i y)^m of one vector, for per-(l, m) solid
 // harmonics and gradients (same recurrences and normalisation as SolidHarmonics).
 template <int L>
@@ -318,14 +333,21 @@ static int resident_blocks(const void* kern, int threads, int smem, int* out) {
 
 template <int L>
 struct ForceDispatch {
-  static int run(const ForceArgs& a, int wpb_tuned, cudaStream_t st) {
+  static int run(const ForceArgs& a, int wpb_tuned, int out_mode, cudaStream_t st) {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     // G = dE/dc
     const int SN = a.S * a.N;
     const int64_t dense_bytes = 4 * (int64_t)(((SN * ((L + 1) * (L + 1) | 1) + 3) & ~3) + (L + 1) * SN * (SN + 1));
-    if (dense_bytes <= 100 * 1024) {
+    if (out_mode == SOAPB_OUT_CC) {
+      const int64_t n = a.n_centres * SN * (L + 1) * (L + 1);
+      int64_t blocks = (n + 255) / 256;
+      if (blocks > (int64_t)nsm * 32) blocks = (int64_t)nsm * 32;
+      k_adjoint_g_cc<<<(unsigned)blocks, 256, 0, st>>>(a, (L + 1) * (L + 1));
+      int rc = check_launch("k_adjoint_g_cc");
+      if (rc) return rc;
+    } else if (dense_bytes <= 100 * 1024) {
       auto kern = k_adjoint_g_dense<L>;
       const int smem = (int)dense_bytes;
       int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
@@ -391,9 +413,12 @@ extern "C" int soapb_forces_workspace(const soapb_basis* b, int64_t n_centres, i
 }
 
 extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
-                            const float* d_coeff, const float* d_dEdp, const int32_t* d_centre_atom, int32_t attach,
-                            float* d_forces, void* d_work, int64_t work_bytes, int32_t* d_counter, void* stream) {
+                            const float* d_coeff, const float* d_dEdp, int32_t out_mode, const int32_t* d_centre_atom,
+                            int32_t attach, float* d_forces, void* d_work, int64_t work_bytes, int32_t* d_counter,
+                            void* stream) {
   if (!b || !b->dev) return set_error(SOAPB_ERR_ARG, "basis not built");
+  if (out_mode != SOAPB_OUT_PS && out_mode != SOAPB_OUT_CC)
+    return set_error(SOAPB_ERR_ARG, "forces: out_mode must be SOAPB_OUT_PS or SOAPB_OUT_CC");
   if (n_centres < 0 || n_centres >= (int64_t)1 << 31) return set_error(SOAPB_ERR_ARG, "bad n_centres");
   if (n_centres == 0) return SOAPB_OK;
   if (!d_pair_off || !d_coeff || !d_dEdp || !d_forces || !d_counter) return set_error(SOAPB_ERR_ARG, "null argument");
@@ -426,5 +451,5 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.inv_h = (float)(1.0 / b->seg_width);
   int rc = check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st), "reset work counter");
   if (rc) return rc;
-  return dispatch_l<ForceDispatch>(b->l_max, a, b->tune[2], st);
+  return dispatch_l<ForceDispatch>(b->l_max, a, b->tune[2], (int)out_mode, st);
 }

@@ -225,13 +225,14 @@ class _SOAPFunction(torch.autograd.Function):
     def forward(ctx, positions, soap, batch, mode):
         pairs = _Pairs(soap, batch, _lib.NL_ALL)
         desc, coeff = soap._run_descriptor(batch, pairs, mode, want_coeff=True)
-        ctx.soap, ctx.batch, ctx.pairs, ctx.coeff = soap, batch, pairs, coeff
+        ctx.soap, ctx.batch, ctx.pairs, ctx.coeff, ctx.mode = soap, batch, pairs, coeff, mode
         return desc
 
     @staticmethod
     def backward(ctx, grad_out):
         soap, batch, pairs = ctx.soap, ctx.batch, ctx.pairs
-        forces = soap._run_forces(batch, pairs, ctx.coeff, grad_out.contiguous().to(torch.float32), attach=True)
+        forces = soap._run_forces(batch, pairs, ctx.coeff, grad_out.contiguous().to(torch.float32), attach=True,
+                                  mode=ctx.mode)
         return (-forces).to(torch.float64), None, None, None
 
 
@@ -317,7 +318,8 @@ class SOAPBatch:
         soap, b, lib = self.soap, self.b, _lib.load()
         self.forces.zero_()
         check(lib.soapb_forces(ctypes.byref(soap._basis), b.n_centres, _ptr(self.pair_off), _ptr(self.pairs),
-                               _ptr(self.coeff), _ptr(self.dEdp), _ptr(b.centre_attach), 1, _ptr(self.forces),
+                               _ptr(self.coeff), _ptr(self.dEdp), _lib.OUT_PS, _ptr(b.centre_attach), 1,
+                               _ptr(self.forces),
                                _ptr(self.fwork), self.fwork.numel(), _ptr(self.counter), _stream(soap.device)))
 
     def _replay_forward(self, positions: Optional[torch.Tensor]):
@@ -654,15 +656,16 @@ class SOAP:
                    _stream(self.device))
         return out, coeff
 
-    def _run_forces(self, batch, pairs, coeff, dEdp, attach=True):
+    def _run_forces(self, batch, pairs, coeff, dEdp, attach=True, mode=None):
         lib = _lib.load()
         forces = torch.zeros((batch.n_atoms, 3), dtype=torch.float32, device=self.device)
         wsb = ctypes.c_int64(0)
         check(lib.soapb_forces_workspace(ctypes.byref(self._basis), batch.n_centres, ctypes.byref(wsb)))
         work = torch.empty(max(int(wsb.value), 256), dtype=torch.uint8, device=self.device)
         self._call("forces", lib.soapb_forces, ctypes.byref(self._basis), batch.n_centres, _ptr(pairs.pair_off),
-                   _ptr(pairs.pairs), _ptr(coeff), _ptr(dEdp), _ptr(batch.centre_attach), int(bool(attach)),
-                   _ptr(forces), _ptr(work), work.numel(), _ptr(self._counter), _stream(self.device))
+                   _ptr(pairs.pairs), _ptr(coeff), _ptr(dEdp), self._out_mode() if mode is None else mode,
+                   _ptr(batch.centre_attach), int(bool(attach)), _ptr(forces), _ptr(work), work.numel(),
+                   _ptr(self._counter), _stream(self.device))
         return forces
 
     def _out_mode(self) -> int:
@@ -707,8 +710,6 @@ class SOAP:
         mode = self._out_mode()
         grad = torch.is_grad_enabled() and any(p.requires_grad for p in batch.pos_tensors)
         if grad:
-            if mode != _lib.OUT_PS:
-                raise NotImplementedError("the adjoint is built for the power spectrum (average != 'cc')")
             if len(batch.pos_tensors) != len(systems):
                 raise ValueError("differentiable create() needs every structure's positions as a tensor")
             pos = batch.pos_tensors[0] if len(batch.pos_tensors) == 1 else torch.cat(batch.pos_tensors)

@@ -236,7 +236,8 @@ int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int64_t* d_pai
                    const int32_t* d_centre_atom, int32_t attach, int32_t max_pairs, int32_t out_mode, float* d_out,
                    void* d_work, int64_t work_bytes, int32_t* d_status, void* stream);
 
-/* Adjoint: given dE/dp (n_centres, n_feat_ps) float32, accumulate
+/* Adjoint: given dE/dp (n_centres, F) float32 of the descriptor of out_mode
+ * (SOAPB_OUT_PS: F = n_feat_ps; SOAPB_OUT_CC: F = n_feat_cc), accumulate
  * d_forces[a] += -dE/dx_a (float32 (n_atoms, 3); the caller zeroes it) with
  * float atomics.  attach = 1: centres move with their atoms (d_centre_atom);
  * 0: fixed centres.  d_coeff: raw coefficients on SOAPB_NL_ALL pairs.
@@ -245,8 +246,9 @@ int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int64_t* d_pai
  * autograd Jacobian SG:2007-2113 without materialising dp/dr. */
 int soapb_forces_workspace(const soapb_basis* b, int64_t n_centres, int64_t* bytes);
 int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
-                 const float* d_coeff, const float* d_dEdp, const int32_t* d_centre_atom, int32_t attach,
-                 float* d_forces, void* d_work, int64_t work_bytes, int32_t* d_counter, void* stream);
+                 const float* d_coeff, const float* d_dEdp, int32_t out_mode, const int32_t* d_centre_atom,
+                 int32_t attach, float* d_forces, void* d_work, int64_t work_bytes, int32_t* d_counter,
+                 void* stream);
 
 /* Message describing the last error on the calling thread ("" if none). */
 const char* soapb_last_error(void);

@@ -665,7 +665,7 @@ class OracleSOAP:
         c = np.zeros((A * S, N * K))
         np.add.at(c, ci * S + sp, (Bl * R[:, None, :]).reshape(-1, N * K))
         c = c.reshape(A, S, N, K)
-        G = self.adjoint_G(c, dEdp)
+        G = self.adjoint_G_cc(dEdp) if self.average == "cc" else self.adjoint_G(c, dEdp)
         Ge = G[ci, sp]  # (E, N, K)
         dEdr = (rv * (Ge * Bhl * R[:, None, :]).sum((1, 2))[:, None]
                 + np.einsum("enk,edk->ed", Ge * Bl, dR))
@@ -674,6 +674,16 @@ class OracleSOAP:
         if attach:
             np.add.at(F, ci, dEdr)
         return F
+
+    def adjoint_G_cc(self, dEdp):
+        """G = dE/dc for E = sum dEdp * cc-projection: the cc layout's
+        permutation and scale (SG:1603-1622) run backwards."""
+        perm, scale = self.cc_perm_scale()
+        C = dEdp.shape[0]
+        D = np.asarray(dEdp, np.float64).reshape(C, self.S, self.n_max, self.K) * scale
+        G = np.zeros_like(D)
+        G[..., perm] = D
+        return G
 
     def adjoint_G(self, c, dEdp):
         """G[c,s,n,lm] = dE/dc[c,s,n,lm] for E = sum dEdp * p (power spectrum)."""

@@ -305,3 +305,22 @@ def test_forces_many_species_vs_oracle():
     E.backward()
     Fo = o.forces(pos, Z, np.tile(w, (n, 1)))
     assert rel_l2(-pt.grad.cpu().numpy(), Fo) < DERIV_TOL
+
+
+@pytest.mark.parametrize("name", ["cluster192", "waterbox2001"])
+def test_forces_cc_vs_oracle(name):
+    """average='cc' is differentiable too: the adjoint runs the cc layout's
+    permutation and scale backwards; forces of E = sum w . cc against the
+    oracle (periodic box included)."""
+    from cusoap_b200 import SOAP
+    P = dict(W.CONFIGS[name], average="cc")
+    sysd = W.make("cluster192") if name == "cluster192" else W.water_box(8, 6.21, seed=5, dmin=2.4)
+    s = SOAP(**P)
+    o = OracleSOAP(**P)
+    w = np.random.default_rng(8).standard_normal(s.get_number_of_features())
+    pt = torch.tensor(sysd["positions"], device="cuda", requires_grad=True)
+    d = dict(sysd, positions=pt)
+    (s.create(d) * torch.tensor(w, dtype=torch.float32, device="cuda")).sum().backward()
+    Fo = o.forces(sysd["positions"], sysd["atomic_numbers"], np.tile(w, (len(sysd["atomic_numbers"]), 1)),
+                  sysd.get("cell"), sysd.get("pbc"))
+    assert rel_l2(-pt.grad.cpu().numpy(), Fo) < DERIV_TOL

@@ -61,7 +61,8 @@ def test_device_entry_points_validate_before_launch():
     lib = _lib.load()
     b = _lib.Basis()
     assert lib.soapb_descriptor(ctypes.byref(b), 10, None, None, 0, None, None, None, None) == _lib.ERR_ARG
-    assert lib.soapb_forces(ctypes.byref(b), 10, None, None, None, None, None, 1, None, None, 0, None, None) == _lib.ERR_ARG
+    assert lib.soapb_forces(ctypes.byref(b), 10, None, None, None, None, 0, None, 1, None, None, 0, None,
+                            None) == _lib.ERR_ARG
 
 
 def test_soap_requires_cuda_device():
