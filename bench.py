@@ -72,23 +72,88 @@ def _traffic_from_profiles():
 
 
 class Clocks:
-    """nvidia-smi sampler for the timed region."""
+    """SM clock and throttle-reason sampler for the timed region.
+
+    Reads NVML (the library behind nvidia-smi) from a background thread every
+    5 ms, on the GPU that this process's CUDA device is (matched by UUID, so a
+    remapped device list cannot point it at another GPU); falls back to an
+    nvidia-smi subprocess.  Only reads; changes no setting."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
+        import threading
         self.index = index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.rows = []
+        self.p = None
+        self.nv = None
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "20"],
-                                      stdout=self.f, stderr=subprocess.DEVNULL)
+            import pynvml as nv
+            import torch
+            nv.nvmlInit()
+            h = None
+            uuid = str(getattr(torch.cuda.get_device_properties(index), "uuid", "") or "")
+            if uuid:
+                try:
+                    h = nv.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+                except Exception:
+                    h = None
+            if h is None:
+                h = nv.nvmlDeviceGetHandleByIndex(index)
+            self.nv, self.h = nv, h
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            bits = {"hw_slowdown": "HwSlowdown", "hw_thermal_slowdown": "HwThermalSlowdown",
+                    "sw_thermal_slowdown": "SwThermalSlowdown", "sw_power_cap": "SwPowerCap"}
+            self.bits = {k: getattr(nv, "nvmlClocksEventReason" + v, None) or getattr(nv, "nvmlClocksThrottleReason" + v)
+                         for k, v in bits.items()}
+            self.stop_ev = threading.Event()
+
+            def run():
+                while not self.stop_ev.is_set():
+                    try:
+                        self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(get(h))))
+                    except Exception:
+                        pass
+                    time.sleep(0.005)
+            self.t = threading.Thread(target=run, daemon=True)
+            self.t.start()
         except Exception:
-            self.p = None
+            self.nv = None
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            try:
+                self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}",
+                                           "--format=csv,noheader,nounits", "-lms", "20"],
+                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            except Exception:
+                self.p = None
+
+    def wait_first_sample(self, timeout_s: float = 5.0):
+        """Block until the first sample exists, so that the timed region that
+        follows is covered from its start."""
+        t0 = time.time()
+        while time.time() - t0 < timeout_s:
+            if self.nv is not None and self.rows:
+                return
+            if self.p is not None and os.path.getsize(self.f.name) > 0:
+                return
+            if self.nv is None and self.p is None:
+                return
+            time.sleep(0.002)
 
     def stop(self):
+        if self.nv is not None:
+            self.stop_ev.set()
+            self.t.join(timeout=2)
+            rows = list(self.rows)
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": ["no samples"], "source": "nvml"}
+            reasons = sorted({k for _, r in rows for k, b in self.bits.items() if r & b})
+            return {"sm_mhz": statistics.median(x for x, _ in rows), "sm_max_mhz": self.smax, "reasons": reasons,
+                    "samples": len(rows), "source": "nvml"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
@@ -111,7 +176,7 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "source": "nvidia-smi"}
 
 
 def _dist():
@@ -379,6 +444,7 @@ def run_ours(args):
 
     # ---- device-resident timed region ----
     clocks = Clocks(torch.cuda.current_device() if world == 1 else local)
+    clocks.wait_first_sample()
     soap.profile = []
     launches0 = _lib.kernel_launches()
     evs = []
@@ -486,7 +552,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)

@@ -256,9 +256,8 @@ class SOAPBatch:
     """
 
     def __init__(self, soap: "SOAP", systems: List[Any], headroom: float = 1.25):
-        if soap.average == "cc":
-            raise NotImplementedError("SOAP.batch is built for the power spectrum (average != 'cc')")
         self.soap = soap
+        self.mode = soap._out_mode()
         self.headroom = float(headroom)
         with torch.cuda.device(soap.device):
             self.b = _Batch(soap, systems, [None] * len(systems))
@@ -283,6 +282,7 @@ class SOAPBatch:
         self.capacity = int(capacity)
         self.pairs = torch.empty((self.capacity, 4), dtype=torch.float32, device=dev)
         F, FC = int(soap._basis.n_feat_ps), int(soap._basis.n_feat_cc)
+        F = FC if self.mode == _lib.OUT_CC else F
         self.desc = torch.empty((C, F), dtype=torch.float32, device=dev)
         self.coeff = torch.empty((C, FC), dtype=torch.float32, device=dev)
         self.dEdp = torch.empty((C, F), dtype=torch.float32, device=dev)
@@ -311,14 +311,14 @@ class SOAPBatch:
         check(lib.soapb_neighbors_fill(bb, cs, cc, _lib.NL_ALL, _ptr(self.work), self.work.numel(),
                                        _ptr(self.pair_off), _ptr(self.pairs), self.capacity, st))
         check(lib.soapb_neighbors_clamp(_ptr(self.pair_off), b.n_centres, self.capacity, _ptr(self.total), st))
-        check(lib.soapb_descriptor(bb, b.n_centres, _ptr(self.pair_off), _ptr(self.pairs), _lib.OUT_PS,
+        check(lib.soapb_descriptor(bb, b.n_centres, _ptr(self.pair_off), _ptr(self.pairs), self.mode,
                                    _ptr(self.desc), _ptr(self.coeff), _ptr(self.counter), st))
 
     def _backward_calls(self):
         soap, b, lib = self.soap, self.b, _lib.load()
         self.forces.zero_()
         check(lib.soapb_forces(ctypes.byref(soap._basis), b.n_centres, _ptr(self.pair_off), _ptr(self.pairs),
-                               _ptr(self.coeff), _ptr(self.dEdp), _lib.OUT_PS, _ptr(b.centre_attach), 1,
+                               _ptr(self.coeff), _ptr(self.dEdp), self.mode, _ptr(b.centre_attach), 1,
                                _ptr(self.forces),
                                _ptr(self.fwork), self.fwork.numel(), _ptr(self.counter), _stream(soap.device)))
 

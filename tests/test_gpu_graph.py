@@ -80,3 +80,44 @@ def test_graph_replans_when_pairs_outgrow_the_buffer():
     ref0 = soap.create(_with_positions(systems, pos0))
     ref0 = torch.cat(ref0) if isinstance(ref0, list) else ref0.reshape(-1, ref0.shape[-1])
     assert torch.equal(got0, ref0)
+
+
+def test_graph_plan_cc_and_ase_like_input():
+    """The plan with average='cc' (forward and adjoint), on ASE-like objects
+    (get_positions / get_atomic_numbers / get_cell / get_pbc)."""
+    from cusoap_b200 import SOAP
+
+    class Atoms:
+        def __init__(self, d):
+            self.d = d
+
+        def get_positions(self):
+            return self.d["positions"]
+
+        def get_atomic_numbers(self):
+            return self.d["atomic_numbers"]
+
+        def get_cell(self):
+            class C:
+                array = np.asarray(self.d["cell"])
+            return C()
+
+        def get_pbc(self):
+            return np.asarray(self.d["pbc"])
+
+    soap = SOAP(**dict(W.CONFIGS["cells512"], average="cc"))
+    cells = _cells(6, seed=12)
+    atoms = [Atoms(c) for c in cells]
+    plan = soap.batch(atoms)
+    w = torch.tensor(np.random.default_rng(3).standard_normal(soap.get_number_of_features()),
+                     dtype=torch.float32, device="cuda")
+    pos = torch.tensor(np.concatenate([c["positions"] for c in cells]), device="cuda", requires_grad=True)
+    out = plan.create(pos)
+    ref = soap.create(atoms)
+    ref = torch.cat(ref) if isinstance(ref, list) else ref.reshape(-1, ref.shape[-1])
+    assert torch.equal(out, ref)
+    (out @ w).sum().backward()
+    pos2 = pos.detach().clone().requires_grad_(True)
+    out2 = soap.create(_with_positions(cells, pos2))
+    ((torch.cat(out2) if isinstance(out2, list) else out2.reshape(-1, out2.shape[-1])) @ w).sum().backward()
+    assert torch.allclose(pos.grad, pos2.grad, rtol=1e-5, atol=1e-6 * float(pos2.grad.abs().max()))
