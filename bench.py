@@ -361,6 +361,42 @@ def run_batched_only(args):
                       "ms_per_step": e0.elapsed_time(e1) / args.steps, "stage_ms_per_step": st}), flush=True)
 
 
+def diff_forces(soap_cls, torch, steps: int = 20, warmup: int = 3):
+    """The differentiation workload: periodic water box of 2001 atoms
+    (667 molecules at 1.0 g/cm^3, 27.1 A cube; n_max 8, l_max 6, sigma 1),
+    E = sum_i w . p_i with seeded N(0, 1) weights, forces from create() and
+    the adjoint (E.backward()); positions resident on the device."""
+    from cusoap_b200 import workloads as W
+    box = W.make("waterbox2001")
+    soap = soap_cls(**W.CONFIGS["waterbox2001"])
+    w = torch.tensor(np.random.default_rng(0).standard_normal(soap.get_number_of_features()),
+                     dtype=torch.float32, device="cuda")
+    pos0 = torch.tensor(box["positions"], dtype=torch.float64, device="cuda")
+
+    def step():
+        pos = pos0.clone().requires_grad_(True)
+        (soap.create(dict(box, positions=pos)) @ w).sum().backward()
+        return pos.grad
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    soap.profile = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    st = {k: v / steps for k, v in soap.stage_times().items()}
+    soap.profile = None
+    ms = e0.elapsed_time(e1) / steps
+    n = len(box["atomic_numbers"])
+    return {"workload": "periodic water box, 2001 atoms, r_cut 6, n_max 8, l_max 6, sigma 1; E = sum w.p, forces "
+                        "by create() + E.backward() (the adjoint)",
+            "atoms_per_s": n / (ms / 1e3), "ms_per_step": ms, "stage_ms_per_step": st}
+
+
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA at the 1965 MHz max clock
 
 
@@ -524,11 +560,16 @@ def run_ours(args):
             extra = {"error": repr(exc)}
 
     scale = None
+    diff = None
     if not args.no_batched and rank == 0 and args.nx == 10:
         try:
             scale = scale_create(SOAP, torch)
         except Exception as exc:  # reported, never silently dropped
             scale = {"error": repr(exc)}
+        try:
+            diff = diff_forces(SOAP, torch)
+        except Exception as exc:
+            diff = {"error": repr(exc)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and args.nx == 10:
@@ -545,7 +586,7 @@ def run_ours(args):
             "config": dict(CONFIG, parallelism=f"replicas x{world}" if world > 1 else "single GPU")
             if args.nx == 10 else {"workload": f"profiling case: {n_at}-atom water cluster, same parameters"},
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk, "cpu_baseline": cpu,
-            "batched_vs_plain": extra, "scale_create": scale}
+            "batched_vs_plain": extra, "scale_create": scale, "diff_forces": diff}
     print(json.dumps(line), flush=True)
 
 
