@@ -186,28 +186,76 @@ def _dist():
     return world, rank, local
 
 
+def parity_centres(n_centres: int = 24):
+    """The sampled centres of the CPU baseline (and of the Jacobian parity check)."""
+    rng = np.random.default_rng(0)
+    return [int(c) for c in rng.choice(3000, n_centres, replace=False)]
+
+
 def cpu_baseline_sample(n_centres: int = 24, workers: int = 1):
     """Oracle (FP64 numpy restatement of the reference path) on a bounded
     sample: create over all 3000 centres plus the dense Jacobian of
-    n_centres centres; scaled to atoms/s of the full step."""
+    n_centres centres; scaled to atoms/s of the full step.  Also returns the
+    oracle's outputs, the checker of the GPU step's parity."""
     from oracle.soap_oracle import OracleSOAP
     from cusoap_b200 import workloads as W
     sysd = W.make(WORKLOAD)
     o = OracleSOAP(**W.CONFIGS[WORKLOAD])
     pos, Z = sysd["positions"], sysd["atomic_numbers"]
     t0 = time.perf_counter()
-    o.create(pos, Z)
+    desc = o.create(pos, Z)
     t_create = time.perf_counter() - t0
-    rng = np.random.default_rng(0)
-    cen = [int(c) for c in rng.choice(3000, n_centres, replace=False)]
+    cen = parity_centres(n_centres)
     t0 = time.perf_counter()
-    o.derivatives(pos, Z, centers=cen, return_descriptor=False)
+    jac = o.derivatives(pos, Z, centers=cen, return_descriptor=False)
     t_der = time.perf_counter() - t0
     per_atom = t_create / 3000 + t_der / n_centres
     return {"value": 1.0 / per_atom, "unit": UNIT, "cores": workers, "kind": "port",
             "sample": f"oracle create of all 3000 centres ({t_create:.2f} s) + dense FP64 Jacobian of "
                       f"{n_centres} sampled centres ({t_der:.2f} s), scaled to one full step",
-            "seconds": t_create + t_der}
+            "seconds": t_create + t_der}, desc, jac
+
+
+def _row_err(a, b) -> float:
+    """Largest relative L2 error over rows (a row = one centre's descriptor or Jacobian block)."""
+    a = np.asarray(a, np.float64).reshape(a.shape[0], -1)
+    b = np.asarray(b, np.float64).reshape(b.shape[0], -1)
+    nb = np.linalg.norm(b, axis=1)
+    return float(np.max(np.linalg.norm(a - b, axis=1) / np.where(nb > 0, nb, 1.0)))
+
+
+def parity_other_legs(soap_cls, torch):
+    """FP64-oracle errors of the batched, scale and differentiation legs'
+    computations (the same calls as the timed legs, on samples: 3 cells, 4
+    centres of the 1M-atom cluster, all forces of the 2001-atom box)."""
+    from oracle.soap_oracle import OracleSOAP, rel_l2
+    from cusoap_b200 import workloads as W
+    out = {}
+    cells = W.make("cells512")[:3]
+    s = soap_cls(**W.CONFIGS["cells512"])
+    o = OracleSOAP(**W.CONFIGS["cells512"])
+    got = s.create(cells)
+    out["batched_desc_max_row_rel_l2"] = max(
+        _row_err(g.cpu().numpy(), o.create(c["positions"], c["atomic_numbers"], cell=c["cell"], pbc=c["pbc"]))
+        for g, c in zip(got, cells))
+    big = W.make("cluster1M")
+    s = soap_cls(**W.CONFIGS["cluster1M"])
+    o = OracleSOAP(**W.CONFIGS["cluster1M"])
+    cen = [0, 123_456, 500_000, 1_000_001]
+    pos = torch.tensor(big["positions"], dtype=torch.float64, device="cuda")
+    got = s.create({"positions": pos, "atomic_numbers": big["atomic_numbers"]})[cen].cpu().numpy()
+    out["scale_desc_max_row_rel_l2"] = _row_err(got, o.create(big["positions"], big["atomic_numbers"], centers=cen))
+    del pos
+    box = W.make("waterbox2001")
+    s = soap_cls(**W.CONFIGS["waterbox2001"])
+    o = OracleSOAP(**W.CONFIGS["waterbox2001"])
+    w = np.random.default_rng(0).standard_normal(s.get_number_of_features())
+    p = torch.tensor(box["positions"], dtype=torch.float64, device="cuda", requires_grad=True)
+    (s.create(dict(box, positions=p)) @ torch.tensor(w, dtype=torch.float32, device="cuda")).sum().backward()
+    Fo = o.forces(box["positions"], box["atomic_numbers"], np.tile(w, (len(box["atomic_numbers"]), 1)),
+                  box["cell"], box["pbc"])
+    out["diff_forces_rel_l2"] = rel_l2(-p.grad.cpu().numpy(), Fo)
+    return out
 
 
 def _ref_worker(args):
@@ -485,17 +533,23 @@ def run_ours(args):
     launches0 = _lib.kernel_launches()
     evs = []
     barrier()
-    for _ in range(args.steps):
+    for i in range(args.steps):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         J, D = step()
         e1.record()
         evs.append((e0, e1))
-        del J, D
+        if i < args.steps - 1:
+            del J, D
     barrier()
     launches = _lib.kernel_launches() - launches0
     clk = clocks.stop()
+    # the last timed step's outputs, kept for the parity check against the oracle
+    want_parity = rank == 0 and world == 1 and not args.no_cpu and args.nx == 10
+    par_J = J[parity_centres()].cpu().numpy() if want_parity else None
+    par_D = D.cpu().numpy() if want_parity else None
+    del J, D
     stage = soap.stage_times()
     soap.profile = None
     t_ms = sum(a.elapsed_time(b) for a, b in evs)
@@ -572,8 +626,19 @@ def run_ours(args):
             diff = {"error": repr(exc)}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu and args.nx == 10:
-        cpu = cpu_baseline_sample()
+    parity = None
+    if want_parity:
+        cpu, o_desc, o_jac = cpu_baseline_sample()
+        parity = {"tolerance": {"descriptor": 1e-5, "derivative": 1e-4},
+                  "headline_desc_max_row_rel_l2": _row_err(par_D, o_desc),
+                  "headline_jacobian_max_centre_rel_l2": _row_err(par_J, o_jac),
+                  "note": "relative L2 against the FP64 oracle: every descriptor row of the last timed step, and the "
+                          "Jacobian blocks of the 24 centres the CPU baseline samples"}
+        del o_desc, o_jac
+        try:
+            parity.update(parity_other_legs(SOAP, torch))
+        except Exception as exc:  # reported, never silently dropped
+            parity["error"] = repr(exc)
 
     if world > 1:
         torch.distributed.barrier()
@@ -586,7 +651,7 @@ def run_ours(args):
             "config": dict(CONFIG, parallelism=f"replicas x{world}" if world > 1 else "single GPU")
             if args.nx == 10 else {"workload": f"profiling case: {n_at}-atom water cluster, same parameters"},
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk, "cpu_baseline": cpu,
-            "batched_vs_plain": extra, "scale_create": scale, "diff_forces": diff}
+            "batched_vs_plain": extra, "scale_create": scale, "diff_forces": diff, "parity_vs_fp64": parity}
     print(json.dumps(line), flush=True)
 
 
