@@ -46,7 +46,8 @@ struct BasisDev {
   const double* poly;  // rx[Q] | wr[Q] | g[N][Q]
   float* tab_b;
   float* tab_bh;
-  float* tabt;     // function-major interleaved copy: [fn][seg][B 8 | D 8]
+  float* tabt_b;   // function-major copies: [fn][seg][8]
+  float* tabt_bh;
   float* selfv;    // w0 B_nl(0) per function fn = l N + n
   int* ftab;
   int* widx;
@@ -277,7 +278,7 @@ __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
         for (int k = 0; k < kNCoef; ++k) { Tprev[k] = Tcur[k]; Tcur[k] = Tnext[k]; }
       }
       float* dst = (which ? a.tab_bh : a.tab_b) + ((size_t)seg * NF + fn) * kNCoef;
-      float* dstt = a.tabt + ((size_t)fn * a.nseg + seg) * 2 * kNCoef + which * kNCoef;
+      float* dstt = (which ? a.tabt_bh : a.tabt_b) + ((size_t)fn * a.nseg + seg) * kNCoef;
       for (int k = 0; k < kNCoef; ++k) dst[k] = dstt[k] = (float)mono[k];
     }
   }
@@ -413,7 +414,8 @@ extern "C" int soapb_basis_plan(soapb_basis* b) {
   b->off_ftab = off; off = align_up(off + 8 * (int64_t)b->n_feat_ps, 256);  // two int tables of F
   b->off_widx = off; off = align_up(off + 4 * (int64_t)(L + 1) * (S * N) * (S * N), 256);
   b->off_err = off; off = align_up(off + 16, 256);
-  b->off_tabt = off; off = align_up(off + 8 * (int64_t)b->n_seg * NF * kNCoef, 256);
+  b->off_tabt_b = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
+  b->off_tabt_bh = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
   b->off_self = off; off = align_up(off + 4 * (int64_t)NF, 256);
   b->off_poly = off;
   if (b->rbf == SOAPB_RBF_POLY) off = align_up(off + 8 * (int64_t)(2 + N) * b->quad_n, 256);
@@ -443,7 +445,8 @@ extern "C" int soapb_basis_build(soapb_basis* b, void* dev_buf, void* stream) {
   a.poly = (const double*)(base + b->off_poly);
   a.tab_b = (float*)(base + b->off_tab_b);
   a.tab_bh = (float*)(base + b->off_tab_bh);
-  a.tabt = (float*)(base + b->off_tabt);
+  a.tabt_b = (float*)(base + b->off_tabt_b);
+  a.tabt_bh = (float*)(base + b->off_tabt_bh);
   a.selfv = (float*)(base + b->off_self);
   a.ftab = (int*)(base + b->off_ftab);
   a.widx = (int*)(base + b->off_widx);

@@ -38,7 +38,8 @@ struct ForceArgs {
   const float* coeff;
   const float* dEdp;
   const int* centre_atom;
-  const float* tabt;     // [fn][seg][B 8 | D 8]; D = d(w B)/dr, Bhat = D / r
+  const float* tabt_b;   // [fn][seg][8]
+  const float* tabt_bh;  // D = d(w B)/dr; Bhat = D / r
   const float* selfv;    // w0 B_nl(0) for r = 0 edges
   const int* widx;
   const int* ftab;       // second half: l-major pair indices of every feature
@@ -249,14 +250,8 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
         for (int n = 0; n < N; ++n) {
           const int fn = l * N + n;
           float cf[kNCoef], ch[kNCoef];
-          {  // function-major, B and D of one (fn, seg) in one 64-byte run
-            const float4* p = reinterpret_cast<const float4*>(a.tabt + ((size_t)fn * nseg + seg) * 2 * kNCoef);
-            const float4 u0 = __ldg(p), u1 = __ldg(p + 1), v0 = __ldg(p + 2), v1 = __ldg(p + 3);
-            cf[0] = u0.x; cf[1] = u0.y; cf[2] = u0.z; cf[3] = u0.w;
-            cf[4] = u1.x; cf[5] = u1.y; cf[6] = u1.z; cf[7] = u1.w;
-            ch[0] = v0.x; ch[1] = v0.y; ch[2] = v0.z; ch[3] = v0.w;
-            ch[4] = v1.x; ch[5] = v1.y; ch[6] = v1.z; ch[7] = v1.w;
-          }
+          load_coef(a.tabt_b, fn, seg, nseg, cf);   // function-major: row fn, column seg
+          load_coef(a.tabt_bh, fn, seg, nseg, ch);
           const float b = self_edge ? __ldg(a.selfv + fn) : horner7(cf, t), h = horner7(ch, t) * inv_r;
           const float* gr = gs + n * KC + l * l;
 #pragma unroll
@@ -438,7 +433,8 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.coeff = d_coeff;
   a.dEdp = d_dEdp;
   a.centre_atom = d_centre_atom;
-  a.tabt = (const float*)((const char*)b->dev + b->off_tabt);
+  a.tabt_b = (const float*)((const char*)b->dev + b->off_tabt_b);
+  a.tabt_bh = (const float*)((const char*)b->dev + b->off_tabt_bh);
   a.selfv = (const float*)((const char*)b->dev + b->off_self);
   a.widx = (const int*)((const char*)b->dev + b->off_widx);
   a.ftab = (const int*)((const char*)b->dev + b->off_ftab);

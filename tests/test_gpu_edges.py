@@ -72,3 +72,47 @@ def test_cartesian_centres_on_and_off_atoms_derivatives():
     J = s.derivatives(sysd, centers=cen, return_descriptor=False).cpu().numpy()
     Jo = o.derivatives(pos, Z, centers=cen, return_descriptor=False)
     assert _row_err(J, Jo) < DERIV_TOL
+
+
+def _periodic_case(kind, seed=0):
+    rng = np.random.default_rng(seed)
+    if kind == "triclinic":
+        cell = np.array([[9.0, 0.0, 0.0], [3.1, 8.2, 0.0], [-2.4, 1.7, 8.8]])
+        pbc = [True, True, True]
+    elif kind == "mixed_pbc":
+        cell = np.array([[10.0, 0.0, 0.0], [0.0, 11.0, 0.0], [0.0, 0.0, 30.0]])
+        pbc = [True, True, False]
+    elif kind == "tiny_cell":
+        cell = np.array([[3.3, 0.0, 0.0], [0.4, 3.1, 0.0], [0.0, 0.6, 3.5]])
+        pbc = [True, True, True]
+    else:  # unwrapped: atoms spread over several cell images
+        cell = np.array([[8.5, 0.0, 0.0], [0.0, 9.5, 0.0], [1.0, 0.0, 9.0]])
+        pbc = [True, True, True]
+    n = 4 if kind == "tiny_cell" else 40
+    frac = rng.uniform(0.0, 1.0, size=(n, 3))
+    if kind == "unwrapped":
+        frac += rng.integers(-2, 3, size=(n, 3))
+    if kind == "mixed_pbc":
+        frac[:, 2] = rng.uniform(0.3, 0.5, size=n)
+    pos = frac @ cell
+    Z = rng.choice([1, 8], size=n)
+    return {"positions": pos, "atomic_numbers": Z, "cell": cell, "pbc": pbc}
+
+
+@pytest.mark.parametrize("kind", ["triclinic", "mixed_pbc", "tiny_cell", "unwrapped"])
+def test_periodic_geometries_vs_oracle(kind):
+    """create, the Jacobian and the adjoint forces on periodic geometries the
+    workloads do not cover, against the oracle's brute-force image sums."""
+    from cusoap_b200 import SOAP
+    P = dict(species=[1, 8], r_cut=4.5, n_max=4, l_max=3, sigma=0.5, periodic=True)
+    s = SOAP(**P)
+    o = OracleSOAP(**P)
+    sysd = _periodic_case(kind)
+    pos, Z, cell, pbc = sysd["positions"], sysd["atomic_numbers"], sysd["cell"], sysd["pbc"]
+    d = s.create(sysd).cpu().numpy()
+    assert _row_err(d, o.create(pos, Z, cell=cell, pbc=pbc)) < DESC_TOL
+    w = np.random.default_rng(1).standard_normal(s.get_number_of_features())
+    pt = torch.tensor(pos, device="cuda", requires_grad=True)
+    (s.create(dict(sysd, positions=pt)) * torch.tensor(w, dtype=torch.float32, device="cuda")).sum().backward()
+    Fo = o.forces(pos, Z, np.tile(w, (len(Z), 1)), cell, pbc)
+    assert rel_l2(-pt.grad.cpu().numpy(), Fo) < DERIV_TOL
