@@ -344,12 +344,12 @@ __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
           int f = s_boff[b];
           for (int n = 0; n < N; ++n)
             for (int nd = (j == jd ? n : 0); nd < N; ++nd) {
-              // second table: l-major coefficient-pair indices (l S + j) N + n, (l S + j') N + n', and l
-              a.ftab[a.F + f] = ((l * S + j) * N + n) | (((l * S + jd) * N + nd) << 12) | (l << 24);
+              // l-major coefficient-pair indices (l S + j) N + n, (l S + j') N + n', and l
+              a.ftab[f] = ((l * S + j) * N + n) | (((l * S + jd) * N + nd) << 12) | (l << 24);
               const int SN = S * N, ia = j * N + n, ib = jd * N + nd;
               a.widx[(l * SN + ib) * SN + ia] = f | (ia == ib ? (1 << 30) : 0);
               a.widx[(l * SN + ia) * SN + ib] = f | (ia == ib ? (1 << 30) : 0);
-              a.ftab[f++] = fcode(j, jd, n, nd, l);
+              ++f;
             }
         }
   }
@@ -411,7 +411,7 @@ extern "C" int soapb_basis_plan(soapb_basis* b) {
   b->off_beta = off; off = align_up(off + 8 * (int64_t)NF * N, 256);
   b->off_tab_b = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
   b->off_tab_bh = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
-  b->off_ftab = off; off = align_up(off + 8 * (int64_t)b->n_feat_ps, 256);  // two int tables of F
+  b->off_ftab = off; off = align_up(off + 4 * (int64_t)b->n_feat_ps, 256);
   b->off_widx = off; off = align_up(off + 4 * (int64_t)(L + 1) * (S * N) * (S * N), 256);
   b->off_err = off; off = align_up(off + 16, 256);
   b->off_tabt_b = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);

@@ -243,9 +243,5 @@ __host__ __device__ inline LaneFns lane_fns(int lane, int N, int L, bool paired)
   return f;
 }
 
-// Packed feature code of the power spectrum table: j | j' << 4 | n << 8 | n' << 13 | l << 18.
-__host__ __device__ inline int fcode(int j, int jd, int n, int nd, int l) {
-  return j | (jd << 4) | (n << 8) | (nd << 13) | (l << 18);
-}
 
 }  // namespace soapb

@@ -42,7 +42,7 @@ struct ForceArgs {
   const float* tabt_bh;  // D = d(w B)/dr; Bhat = D / r
   const float* selfv;    // w0 B_nl(0) for r = 0 edges
   const int* widx;
-  const int* ftab;       // second half: l-major pair indices of every feature
+  const int* ftab;       // l-major pair indices of every feature
   float* G;              // (n_centres, S N K) workspace
   float* forces;
   int* counter;
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(kGThreads) k_adjoint_g_dense(ForceArgs a) {
       for (int i = threadIdx.x; i < wn; i += blockDim.x) s_W[i] = 0.0f;
     __syncthreads();
     for (int f = threadIdx.x; f < F; f += blockDim.x) {
-      const int code = __ldg(a.ftab + F + f);
+      const int code = __ldg(a.ftab + f);
       const int l = code >> 24, base = l * SN;
       const int ia = (code & 0xfff) - base, ib = ((code >> 12) & 0xfff) - base;
       const float w = wrow[f] * sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * l + 1.0f));

@@ -312,11 +312,11 @@ __device__ __forceinline__ void quad_values(const JacArgs& a, const float* ed, i
   if (a.mode == SOAPB_OUT_PS) {
     int code[4];
     if ((F & 3) == 0) {
-      const int4 c4 = __ldg(reinterpret_cast<const int4*>(a.ftab + F) + q);  // pre-decoded: ia | ib << 12 | l << 24
+      const int4 c4 = __ldg(reinterpret_cast<const int4*>(a.ftab) + q);  // pre-decoded: ia | ib << 12 | l << 24
       code[0] = c4.x; code[1] = c4.y; code[2] = c4.z; code[3] = c4.w;
     } else {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) code[k] = (4 * q + k < F) ? __ldg(a.ftab + F + 4 * q + k) : 0;
+      for (int k = 0; k < 4; ++k) code[k] = (4 * q + k < F) ? __ldg(a.ftab + 4 * q + k) : 0;
     }
     for (int i = g0; i < g1; ++i) {
       const float4* X = reinterpret_cast<const float4*>(ed + (size_t)i * EF + XO);
