@@ -39,7 +39,7 @@ class Basis(ctypes.Structure):
         ("bytes", c_int64),
         ("off_alpha", c_int64), ("off_beta", c_int64), ("off_tab_b", c_int64), ("off_tab_bh", c_int64),
         ("off_ftab", c_int64), ("off_widx", c_int64), ("off_err", c_int64),
-        ("off_tabt_b", c_int64), ("off_tabt_bh", c_int64), ("off_self", c_int64), ("off_poly", c_int64),
+        ("off_tabf", c_int64), ("off_self", c_int64), ("off_poly", c_int64),
         ("dev", c_void_p),
     ]
 

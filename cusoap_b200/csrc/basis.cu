@@ -46,8 +46,7 @@ struct BasisDev {
   const double* poly;  // rx[Q] | wr[Q] | g[N][Q]
   float* tab_b;
   float* tab_bh;
-  float* tabt_b;   // function-major copies: [fn][seg][8]
-  float* tabt_bh;
+  float* tabf;     // function-major [fn][2 nseg][8]: w B on half-width segments
   float* selfv;    // w0 B_nl(0) per function fn = l N + n
   int* ftab;
   int* widx;
@@ -168,6 +167,28 @@ __device__ void exact_BD(const BasisDev& a, const double* s_gamma, const double*
   D = dw * b + w * r * bh;
 }
 
+// Interpolant through the values f_j at the 8 Chebyshev nodes t_j of a
+// segment, as float monomial coefficients in the local coordinate t.
+__device__ void cheb_to_mono(const double (&f)[kNCoef], float* dst) {
+  double cheb[kNCoef];
+  for (int i = 0; i < kNCoef; ++i) {
+    double s = 0.0;
+    for (int j = 0; j < kNCoef; ++j) s += f[j] * cos(i * (2.0 * j + 1.0) * kPi / (2.0 * kNCoef));
+    cheb[i] = s * 2.0 / kNCoef;
+  }
+  cheb[0] *= 0.5;
+  // monomial coefficients: sum_i cheb_i T_i(t), T_{i+1} = 2 t T_i - T_{i-1}
+  double mono[kNCoef] = {0}, Tprev[kNCoef] = {0}, Tcur[kNCoef] = {0}, Tnext[kNCoef];
+  Tcur[0] = 1.0;  // T_0
+  for (int i = 0; i < kNCoef; ++i) {
+    for (int k = 0; k < kNCoef; ++k) mono[k] += cheb[i] * Tcur[k];
+    for (int k = 0; k < kNCoef; ++k)
+      Tnext[k] = (i == 0) ? (k == 1 ? 1.0 : 0.0) : (k > 0 ? 2.0 * Tcur[k - 1] : 0.0) - Tprev[k];
+    for (int k = 0; k < kNCoef; ++k) { Tprev[k] = Tcur[k]; Tcur[k] = Tnext[k]; }
+  }
+  for (int k = 0; k < kNCoef; ++k) dst[k] = (float)mono[k];
+}
+
 __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
   const int N = a.N, L = a.L, NF = N * (L + 1);
   __shared__ double s_gamma[(kMaxL + 1) * kMaxN];
@@ -259,28 +280,22 @@ __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
       const double r = (seg + 0.5 * (tj + 1.0)) * a.h;
       exact_BD(a, s_gamma, s_pref, fn, r, fb[j], fh[j]);
     }
-    for (int which = 0; which < 2; ++which) {
-      const double* f = which ? fh : fb;
-      double cheb[kNCoef];
-      for (int i = 0; i < kNCoef; ++i) {
-        double s = 0.0;
-        for (int j = 0; j < kNCoef; ++j) s += f[j] * cos(i * (2.0 * j + 1.0) * kPi / (2.0 * kNCoef));
-        cheb[i] = s * 2.0 / kNCoef;
-      }
-      cheb[0] *= 0.5;
-      // monomial coefficients: sum_i cheb_i T_i(t), T_{i+1} = 2 t T_i - T_{i-1}
-      double mono[kNCoef] = {0}, Tprev[kNCoef] = {0}, Tcur[kNCoef] = {0}, Tnext[kNCoef];
-      Tcur[0] = 1.0;  // T_0
-      for (int i = 0; i < kNCoef; ++i) {
-        for (int k = 0; k < kNCoef; ++k) mono[k] += cheb[i] * Tcur[k];
-        for (int k = 0; k < kNCoef; ++k)
-          Tnext[k] = (i == 0) ? (k == 1 ? 1.0 : 0.0) : (k > 0 ? 2.0 * Tcur[k - 1] : 0.0) - Tprev[k];
-        for (int k = 0; k < kNCoef; ++k) { Tprev[k] = Tcur[k]; Tcur[k] = Tnext[k]; }
-      }
-      float* dst = (which ? a.tab_bh : a.tab_b) + ((size_t)seg * NF + fn) * kNCoef;
-      float* dstt = (which ? a.tabt_bh : a.tabt_b) + ((size_t)fn * a.nseg + seg) * kNCoef;
-      for (int k = 0; k < kNCoef; ++k) dst[k] = dstt[k] = (float)mono[k];
+    cheb_to_mono(fb, a.tab_b + ((size_t)seg * NF + fn) * kNCoef);
+    cheb_to_mono(fh, a.tab_bh + ((size_t)seg * NF + fn) * kNCoef);
+  }
+  // Force table: w B alone on segments of half the width, function-major; its
+  // polynomial's derivative is D (the derivative of a degree-7 interpolant
+  // loses about h per order, halving h wins back 2^7).
+  for (int task = tid; task < 2 * a.nseg * NF; task += blockDim.x) {
+    const int seg = task % (2 * a.nseg), fn = task / (2 * a.nseg);
+    double f[kNCoef];
+    for (int j = 0; j < kNCoef; ++j) {
+      const double tj = cos((2.0 * j + 1.0) * kPi / (2.0 * kNCoef));
+      const double r = (seg + 0.5 * (tj + 1.0)) * (0.5 * a.h);
+      double d;
+      exact_BD(a, s_gamma, s_pref, fn, r, f[j], d);
     }
+    cheb_to_mono(f, a.tabf + ((size_t)fn * 2 * a.nseg + seg) * kNCoef);
   }
   // self values: the centre's own Gaussian, w0 B_nl(0) (SG:765-819)
   for (int fn = tid; fn < NF; fn += blockDim.x) {
@@ -292,7 +307,8 @@ __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
   __syncthreads();
 
   // Table error: max |table - exact| / max |exact| per function, 17 points per
-  // segment over [0, cutoff].
+  // segment over [0, cutoff]; err[0] covers B (both tables), err[1] D (the D
+  // table and the force table's derivative).
   for (int fn = tid; fn < NF; fn += blockDim.x) {
     double eb = 0.0, eh = 0.0, mb = 0.0, mh = 0.0;
     for (int seg = 0; seg < a.nseg; ++seg) {
@@ -310,6 +326,24 @@ __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
         eh = fmax(eh, fabs(ph - bh));
         mb = fmax(mb, fabs(b));
         mh = fmax(mh, fabs(bh));
+      }
+    }
+    // the force table: value, and derivative d/dr = (4 / h) d/dt
+    for (int seg = 0; seg < 2 * a.nseg; ++seg) {
+      const float* cf = a.tabf + ((size_t)fn * 2 * a.nseg + seg) * kNCoef;
+      for (int j = 0; j <= 16; ++j) {
+        const double t = -1.0 + j / 8.0;
+        const double r = (seg + 0.5 * (t + 1.0)) * (0.5 * a.h);
+        if (r > a.cutoff) continue;
+        double b, bh;
+        exact_BD(a, s_gamma, s_pref, fn, r, b, bh);
+        double p = cf[kDeg], dp = 0.0;
+        for (int k = kDeg - 1; k >= 0; --k) {
+          dp = dp * t + p;
+          p = p * t + cf[k];
+        }
+        eb = fmax(eb, fabs(p - b));
+        eh = fmax(eh, fabs(dp * 4.0 / a.h - bh));
       }
     }
     atomic_max_nonneg(&a.err[0], mb > 0 ? eb / mb : 0.0);
@@ -414,8 +448,7 @@ extern "C" int soapb_basis_plan(soapb_basis* b) {
   b->off_ftab = off; off = align_up(off + 4 * (int64_t)b->n_feat_ps, 256);
   b->off_widx = off; off = align_up(off + 4 * (int64_t)(L + 1) * (S * N) * (S * N), 256);
   b->off_err = off; off = align_up(off + 16, 256);
-  b->off_tabt_b = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
-  b->off_tabt_bh = off; off = align_up(off + 4 * (int64_t)b->n_seg * NF * kNCoef, 256);
+  b->off_tabf = off; off = align_up(off + 4 * (int64_t)2 * b->n_seg * NF * kNCoef, 256);
   b->off_self = off; off = align_up(off + 4 * (int64_t)NF, 256);
   b->off_poly = off;
   if (b->rbf == SOAPB_RBF_POLY) off = align_up(off + 8 * (int64_t)(2 + N) * b->quad_n, 256);
@@ -445,8 +478,7 @@ extern "C" int soapb_basis_build(soapb_basis* b, void* dev_buf, void* stream) {
   a.poly = (const double*)(base + b->off_poly);
   a.tab_b = (float*)(base + b->off_tab_b);
   a.tab_bh = (float*)(base + b->off_tab_bh);
-  a.tabt_b = (float*)(base + b->off_tabt_b);
-  a.tabt_bh = (float*)(base + b->off_tabt_bh);
+  a.tabf = (float*)(base + b->off_tabf);
   a.selfv = (float*)(base + b->off_self);
   a.ftab = (int*)(base + b->off_ftab);
   a.widx = (int*)(base + b->off_widx);

@@ -48,6 +48,17 @@ __device__ __forceinline__ float horner7(const float (&a)[kNCoef], float t) {
   return p;
 }
 
+// Value p and derivative dp/dt of the degree-7 segment polynomial in one pass.
+__device__ __forceinline__ void horner7_d(const float (&a)[kNCoef], float t, float& p, float& dp) {
+  p = a[7];
+  dp = 0.0f;
+#pragma unroll
+  for (int k = kDeg - 1; k >= 0; --k) {
+    dp = fmaf(dp, t, p);
+    p = fmaf(p, t, a[k]);
+  }
+}
+
 __device__ __forceinline__ void load_coef(const float* __restrict__ tab, int seg, int fn, int NF,
                                           float (&a)[kNCoef]) {
   const float4* p = reinterpret_cast<const float4*>(tab + ((size_t)seg * NF + fn) * kNCoef);

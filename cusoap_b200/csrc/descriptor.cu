@@ -37,10 +37,31 @@ struct DescArgs {
   float inv_h;
 };
 
+// Position of harmonic block l in a pair's Y row: l^2 plus a padding that
+// starts every block on a different shared-memory bank (the lane groups of the
+// l blocks read the same slot m of their blocks at once: no conflicts).  Plain
+// l^2 puts l = 6 on the bank of l = 2 (36 = 4 mod 32) and l = 8 on that of
+// l = 0; one float of padding from l = 6 and another from l = 8 separate them.
+__host__ __device__ constexpr int ybase(int l) { return l * l + (l >= 6) + (l >= 8); }
+// Y row position of harmonic index idx = l^2 + l + m (idx >= 36 is l >= 6, idx >= 64 is l >= 8).
+__host__ __device__ constexpr int ypos(int idx) { return idx + (idx >= 36) + (idx >= 64); }
+
+constexpr bool ybase_banks_distinct() {
+  for (int l = 0; l <= kMaxL; ++l) {
+    if (l > 0 && ybase(l) < ybase(l - 1) + 2 * l - 1) return false;  // blocks overlap
+    for (int k = 0; k < l; ++k)
+      if (ybase(k) % 32 == ybase(l) % 32) return false;
+    for (int m = 0; m <= 2 * l; ++m)
+      if (ypos(l * l + m) != ybase(l) + m) return false;
+  }
+  return true;
+}
+static_assert(ybase_banks_distinct(), "Y row blocks must start on distinct banks");
+
 template <int L>
 struct DescShape {
   static constexpr int K = (L + 1) * (L + 1);
-  static constexpr int YS = K | 1;  // odd strides: conflict-free shared-memory rows
+  static constexpr int YS = (ybase(L) + 2 * L + 1) | 1;  // odd strides: conflict-free row writes
   static constexpr int KC = K | 1;
   __host__ __device__ static int warp_floats(int S, int N) { return 32 * YS + 96 + S * N * KC; }
 };
@@ -91,6 +112,7 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
   const bool active = l_me <= L && k_me * GN < N;
   const int lme = active ? l_me : 0;
   const int mme = 2 * lme + 1;
+  const int ybm = ybase(lme);
   float selfb[GN];
 #pragma unroll
   for (int g = 0; g < GN; ++g) {
@@ -150,7 +172,7 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
         sg[lane] = seg;
         spp[lane] = (int)((unsigned)w >> kAtomBits);
         float* yrow = Y + lane * YS;
-        SolidHarmonics<L>::values(pr.x, pr.y, pr.z, [&](int idx, float v) { yrow[idx] = v; });
+        SolidHarmonics<L>::values(pr.x, pr.y, pr.z, [&](int idx, float v) { yrow[ypos(idx)] = v; });
       }
       __syncwarp();
       for (int q = 0; q < nt; ++q) {
@@ -174,10 +196,10 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
         float B[GN];
 #pragma unroll
         for (int g = 0; g < GN; ++g) B[g] = (t > 2.0f) ? selfb[g] : horner7(cf[g], t);
-        // all M slots, without a per-lane test: slots m >= 2l+1 read the next
-        // harmonics of the row (index <= l^2 + 2L < K, in bounds) and collect
+        // all M slots, without a per-lane test: slots m >= 2l+1 read on along
+        // the row (position <= ybase(l) + 2L < YS, in bounds) and collect
         // values that flush() never stores, so no branch is needed per slot
-        const float* yr = Y + q * YS + lme * lme;
+        const float* yr = Y + q * YS + ybm;
 #pragma unroll
         for (int m = 0; m < M; ++m) {
           const float yv = yr[m];

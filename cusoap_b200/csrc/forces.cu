@@ -13,14 +13,18 @@
 //   F[neighbour] -= dE/drvec_e, and with attach F[centre atom] += dE/drvec_e
 //   (centres move with their atoms; self and own-image edges cancel).
 //
-// Two kernels:
-//  k_adjoint_g  one block per centre: dE/dp row and coefficient row staged in
-//               shared memory (coalesced), G[a, lm] computed by thread-tasks
-//               (a, l); the pair {a, b} -> feature map is a per-basis index
-//               table (bit 30 marks a = b).  G goes to the workspace.
+// Two stages:
+//  k_adjoint_g_pipe  one block per centre iteration: the centre's dE/dp and
+//               coefficient rows arrive in shared memory by double-buffered
+//               TMA bulk copies, dE/dp is scattered into dense W_l and G[a, lm]
+//               is computed by thread-tasks (a, l).  G goes to the workspace.
+//               (k_adjoint_g, with a per-basis pair -> feature index table and
+//               no dense W, serves bases whose W does not fit.)
 //  k_forces     one warp per centre (atomic work queue), ONE edge per lane:
-//               the lane evaluates its edge's radial functions B_nl, Bhat_nl
-//               from the function-major copy of the tables (lanes on nearby
+//               the lane evaluates its edge's radial functions B_nl and
+//               Bhat_nl = (dB_nl/dr) / r from one function-major table of
+//               w B on half-width segments (value and derivative of the
+//               segment polynomial in one Horner pass; lanes on nearby
 //               segments share cache lines), its solid harmonics in registers,
 //               and contracts l by l:
 //                 xi_lm = sum_n G[s, n, lm] B_nl, zeta_lm = sum_n G[s, n, lm] Bhat_nl,
@@ -38,8 +42,7 @@ struct ForceArgs {
   const float* coeff;
   const float* dEdp;
   const int* centre_atom;
-  const float* tabt_b;   // [fn][seg][8]
-  const float* tabt_bh;  // D = d(w B)/dr; Bhat = D / r
+  const float* tabf;     // [fn][nsegf][8]: w B on half-width segments; its derivative is D = d(w B)/dr
   const float* selfv;    // w0 B_nl(0) for r = 0 edges
   const int* widx;
   const int* ftab;       // l-major pair indices of every feature
@@ -47,8 +50,8 @@ struct ForceArgs {
   float* forces;
   int* counter;
   int64_t n_centres;
-  int N, S, nseg, F, attach, crossover;
-  float inv_h;
+  int N, S, nsegf, F, attach, crossover;
+  float inv_hf;  // 1 / width of a force-table segment
 };
 
 constexpr int kGThreads = 256;
@@ -97,73 +100,213 @@ __global__ void __launch_bounds__(kGThreads) k_adjoint_g(ForceArgs a) {
   }
 }
 
-// G = dE/dc for one centre per block iteration, W dense in shared memory:
-// the dE/dp row is scattered into W_l[a][b] (both triangles, 2x on a = b,
-// times pref_l) through the l-major pair table, then G[a, lm] = sum_b
-// W_l[a][b] c[b, lm] with lanes over a (W rows padded to SN + 1 floats:
-// conflict-free) and c broadcast.  Used while (L+1) SN (SN+1) floats fit.
-// One G task (a, l) with l known at compile time: G[a, l^2 .. l^2 + 2l] = sum_b W_l[a][b] c[b, lm].
-template <int L, int l>
-__device__ __forceinline__ void g_task(const float* Wr, const float* s_c, int SN, float* grow) {
-  constexpr int K = (L + 1) * (L + 1), KC = K | 1, M = 2 * l + 1;
-  float g[M];
-#pragma unroll
-  for (int m = 0; m < M; ++m) g[m] = 0.0f;
-#pragma unroll 4
-  for (int bi = 0; bi < SN; ++bi) {
-    const float w = Wr[bi];
-    const float* cr = s_c + bi * KC + l * l;
-#pragma unroll
-    for (int m = 0; m < M; ++m) g[m] = fmaf(w, cr[m], g[m]);
-  }
-#pragma unroll
-  for (int m = 0; m < M; ++m) grow[l * l + m] = g[m];
-}
+// G = dE/dc, one centre per block iteration, W dense in shared memory.
+//  - The centre's dE/dp row and coefficient row are brought into shared
+//    memory by TMA bulk copies (cp.async.bulk, completion on an mbarrier),
+//    double-buffered: the next centre's rows are in flight while this one
+//    is computed.  BULK = false (rows not 16-byte aligned) loads them with
+//    plain coalesced loads instead.
+//  - The dE/dp row is scattered into W_l[a][b] (both triangles, 2x on a = b)
+//    through per-block shared-memory indices built once from the l-major
+//    pair table; W rows are padded to SN + 1 floats (conflict-free reads by
+//    lanes over a).  Entries without a feature stay zero.
+//  - The coefficient row is repacked with every l block on a float4
+//    boundary, so G[a, lm] = pref_l sum_b W_l[a][b] c[b, lm] runs as equal
+//    tasks (a, quad of 4 m slots), c read as float4 broadcasts.
+//  - G goes through shared memory to coalesced row stores.
+// Coefficient row layout of the G kernel: l block l starts at off(l), a multiple of 4.
+template <int L>
+struct GRow {
+  static constexpr int K = (L + 1) * (L + 1);
+  __host__ __device__ static constexpr int off(int l) { return l == 0 ? 0 : off(l - 1) + ((2 * l - 1 + 3) & ~3); }
+  static constexpr int KP = off(L + 1);
+};
 
-template <int L, int l = 0>
-__device__ __forceinline__ void g_task_l(int lr, const float* Wr, const float* s_c, int SN, float* grow) {
-  if constexpr (l <= L) {
-    if (lr == l) g_task<L, l>(Wr, s_c, SN, grow);
-    else g_task_l<L, l + 1>(lr, Wr, s_c, SN, grow);
-  }
-}
+// Shared-memory carve-up of k_adjoint_g_pipe in floats (each part a multiple of 4).
+struct GLayout {
+  int idx, w, craw, cp, W, G, total, fa, snka;
+};
 
 template <int L>
-__global__ void __launch_bounds__(kGThreads) k_adjoint_g_dense(ForceArgs a) {
-  constexpr int K = (L + 1) * (L + 1), KC = K | 1;
+__host__ __device__ inline GLayout g_layout(int F, int SN, int nbuf) {
+  constexpr int K = GRow<L>::K, KP = GRow<L>::KP, KG = K | 1;
+  GLayout g;
+  g.fa = (F + 3) & ~3;
+  g.snka = (SN * K + 3) & ~3;
+  g.idx = 0;
+  g.w = g.idx + g.fa;
+  g.craw = g.w + nbuf * g.fa;
+  g.cp = g.craw + nbuf * g.snka;
+  g.W = g.cp + SN * KP;
+  g.G = g.W + (((L + 1) * SN * (SN + 1) + 3) & ~3);
+  g.total = g.G + ((SN * KG + 3) & ~3);
+  return g;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// One TMA bulk copy global -> shared, completing `bytes` on the mbarrier
+// (both addresses 16-byte aligned, bytes a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(void* s, const void* g, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(s)),
+               "l"(g), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Waits for the phase of the given parity to complete; gives up after about
+// one second (global timer) and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  uint64_t t0, t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 > 1000000000ull) return false;
+  }
+}
+
+template <int L, bool BULK>
+__global__ void __launch_bounds__(kGThreads) k_adjoint_g_pipe(ForceArgs a) {
+  constexpr int K = GRow<L>::K, KP = GRow<L>::KP, KG = K | 1;
   extern __shared__ __align__(16) float sm[];
-  const int N = a.N, S = a.S, SN = S * N, WS = SN + 1, F = a.F;
-  float* s_c = sm;                              // SN x KC
-  float* s_W = sm + ((SN * KC + 3) & ~3);       // (L+1) x SN x WS
-  const int wn = (L + 1) * SN * WS;
-  for (int64_t c = blockIdx.x; c < a.n_centres; c += gridDim.x) {
-    const float* wrow = a.dEdp + (size_t)c * F;
-    const float* crow = a.coeff + (size_t)c * SN * K;
-    for (int i = threadIdx.x; i < SN * K; i += blockDim.x) s_c[(i / K) * KC + (i % K)] = crow[i];
-    // with crossover every (a, b, l) has a feature and is written below
-    if (!a.crossover)
-      for (int i = threadIdx.x; i < wn; i += blockDim.x) s_W[i] = 0.0f;
-    __syncthreads();
-    for (int f = threadIdx.x; f < F; f += blockDim.x) {
-      const int code = __ldg(a.ftab + f);
-      const int l = code >> 24, base = l * SN;
-      const int ia = (code & 0xfff) - base, ib = ((code >> 12) & 0xfff) - base;
-      const float w = wrow[f] * sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * l + 1.0f));
-      float* Wl = s_W + (size_t)l * SN * WS;
-      if (ia == ib) {
-        Wl[ia * WS + ia] = 2.0f * w;
-      } else {
-        Wl[ia * WS + ib] = w;
-        Wl[ib * WS + ia] = w;
+  __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ float s_pref[L + 1];
+  __shared__ int s_lmoff[K];
+  __shared__ int s_quad[KP / 4];  // l | (first m) << 8 of every float4 quad of the padded row
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int N = a.N, SN = a.S * N, WS = SN + 1, F = a.F, SNK = SN * K;
+  const GLayout ly = g_layout<L>(F, SN, BULK ? 2 : 1);
+  int* s_idx = reinterpret_cast<int*>(sm + ly.idx);
+  float* s_cp = sm + ly.cp;
+  float* s_W = sm + ly.W;
+  float* s_G = sm + ly.G;
+
+  // once per block: zero W and the padded row, W indices of every feature
+  for (int i = tid; i < ly.total - ly.cp; i += nth) s_cp[i] = 0.0f;  // cp, W and G parts
+  for (int f = tid; f < F; f += nth) {
+    const int code = __ldg(a.ftab + f);
+    const int l = code >> 24, base = l * SN;
+    const int ia = (code & 0xfff) - base, ib = ((code >> 12) & 0xfff) - base;
+    s_idx[f] = ((base + ia) * WS + ib) | (((base + ib) * WS + ia) << 16);
+  }
+  if (tid <= L) s_pref[tid] = sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * tid + 1.0f));
+  for (int lm = tid; lm < K; lm += nth) {
+    int l = 0;
+    while ((l + 1) * (l + 1) <= lm) ++l;
+    s_lmoff[lm] = GRow<L>::off(l) + lm - l * l;
+  }
+  for (int q = tid; q < KP / 4; q += nth) {
+    int l = 0;
+    while (GRow<L>::off(l + 1) <= 4 * q) ++l;
+    s_quad[q] = l | ((4 * q - GRow<L>::off(l)) << 8);
+  }
+  if (tid == 0) {
+    s_fail = 0;
+    if (BULK) {
+      mbar_init(&s_bar[0], 1);
+      mbar_init(&s_bar[1], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+  }
+  __syncthreads();
+
+  const uint32_t bytes_w = 4u * (uint32_t)F, bytes_c = 4u * (uint32_t)SNK;
+  auto issue = [&](int64_t c, int buf) {  // thread 0: both rows of centre c into buffer buf
+    mbar_expect_tx(&s_bar[buf], bytes_w + bytes_c);
+    bulk_g2s(sm + ly.w + buf * ly.fa, a.dEdp + c * F, bytes_w, &s_bar[buf]);
+    bulk_g2s(sm + ly.craw + buf * ly.snka, a.coeff + c * SNK, bytes_c, &s_bar[buf]);
+  };
+  if (BULK && tid == 0 && (int64_t)blockIdx.x < a.n_centres) issue(blockIdx.x, 0);
+
+  int it = 0;
+  for (int64_t c = blockIdx.x; c < a.n_centres; c += gridDim.x, ++it) {
+    const int buf = BULK ? (it & 1) : 0;
+    const float* w_row = sm + ly.w + buf * ly.fa;
+    const float* c_row = sm + ly.craw + buf * ly.snka;
+    bool next = false;
+    if (BULK) {
+      next = c + gridDim.x < a.n_centres;
+      if (tid == 0 && next) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // earlier reads of buf ^ 1 first
+        issue(c + gridDim.x, buf ^ 1);
       }
+      if (!mbar_wait(&s_bar[buf], (it >> 1) & 1)) s_fail = 1;
+    } else {
+      float* w_dst = sm + ly.w;
+      float* c_dst = sm + ly.craw;
+      for (int f = tid; f < F; f += nth) w_dst[f] = a.dEdp[c * F + f];
+      for (int i = tid; i < SNK; i += nth) c_dst[i] = a.coeff[c * SNK + i];
     }
     __syncthreads();
-    float* grow = a.G + (size_t)c * SN * K;
-    for (int t = threadIdx.x; t < SN * (L + 1); t += blockDim.x) {
-      const int l = L - t / SN, ai = t % SN;
-      g_task_l<L>(l, s_W + ((size_t)l * SN + ai) * WS, s_c, SN, grow + ai * K);
+    if (s_fail) {  // a row copy never completed: G of this block's centres is NaN
+      if (BULK && tid == 0 && next) mbar_wait(&s_bar[buf ^ 1], ((it + 1) >> 1) & 1);
+      for (int64_t cc = c; cc < a.n_centres; cc += gridDim.x)
+        for (int i = tid; i < SNK; i += nth) a.G[cc * SNK + i] = __int_as_float(0x7fc00000);
+      return;
+    }
+#pragma unroll 4
+    for (int f = tid; f < F; f += nth) {
+      const int idx = s_idx[f];
+      const int ab = idx & 0xffff, ba = idx >> 16;
+      const float v = w_row[f] * (ab == ba ? 2.0f : 1.0f);
+      s_W[ab] = v;
+      s_W[ba] = v;
+    }
+#pragma unroll 4
+    for (int i = tid; i < SNK; i += nth) {
+      const int bi = i / K;
+      s_cp[bi * KP + s_lmoff[i - bi * K]] = c_row[i];
     }
     __syncthreads();
+    // tasks (a, quad): G[a, l^2 + m0 .. m0 + 3] = pref_l sum_b W_l[a][b] c[b, quad], the
+    // quad read as one float4 (lanes over a share it); padding lanes are not stored
+    for (int t = tid; t < SN * (KP / 4); t += nth) {
+      const int qd = t / SN, ai = t - qd * SN;
+      const int info = s_quad[qd], l = info & 255, m0 = info >> 8;
+      const float* Wr = s_W + (l * SN + ai) * WS;
+      const float4* cq = reinterpret_cast<const float4*>(s_cp) + qd;
+      float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll 8
+      for (int bi = 0; bi < SN; ++bi) {
+        const float w = Wr[bi];
+        const float4 v = cq[bi * (KP / 4)];
+        g.x = fmaf(w, v.x, g.x);
+        g.y = fmaf(w, v.y, g.y);
+        g.z = fmaf(w, v.z, g.z);
+        g.w = fmaf(w, v.w, g.w);
+      }
+      const float p = s_pref[l];
+      const int M = 2 * l + 1;
+      float* go = s_G + ai * KG + l * l + m0;
+      go[0] = p * g.x;
+      if (m0 + 1 < M) go[1] = p * g.y;
+      if (m0 + 2 < M) go[2] = p * g.z;
+      if (m0 + 3 < M) go[3] = p * g.w;
+    }
+    __syncthreads();
+    float* grow = a.G + c * SNK;
+#pragma unroll 4
+    for (int i = tid; i < SNK; i += nth) {
+      const int bi = i / K;
+      grow[i] = s_G[bi * KG + i - bi * K];
+    }
   }
 }
 
@@ -213,7 +356,7 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
   constexpr int K = Sh::K, KC = Sh::KC;
   extern __shared__ __align__(16) float sm[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int N = a.N, SN = a.S * N, nseg = a.nseg;
+  const int N = a.N, SN = a.S * N, nsegf = a.nsegf;
   float* G = sm + (size_t)wid * Sh::warp_floats(a.S, N);
 
   for (;;) {
@@ -236,9 +379,9 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
       int seg;
       float t;
       const float r = sqrtf(x * x + y * y + z * z);
-      seg_coord(r, a.inv_h, nseg, seg, t);
+      seg_coord(r, a.inv_hf, nsegf, seg, t);
       const bool self_edge = !(r > 0.0f);
-      const float inv_r = self_edge ? 0.0f : 1.0f / r;
+      const float dt_r = self_edge ? 0.0f : 2.0f * a.inv_hf / r;  // (dt/dr) / r: Bhat = D / r = dP/dt dt_r
       const EdgeHarmonics<L> eh(x, y, z);
       const float* gs = G + sp * N * KC;
       float ex = 0.f, ey = 0.f, ez = 0.f;
@@ -249,10 +392,11 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
         for (int m = 0; m < 2 * l + 1; ++m) { xi[m] = 0.0f; ze[m] = 0.0f; }
         for (int n = 0; n < N; ++n) {
           const int fn = l * N + n;
-          float cf[kNCoef], ch[kNCoef];
-          load_coef(a.tabt_b, fn, seg, nseg, cf);   // function-major: row fn, column seg
-          load_coef(a.tabt_bh, fn, seg, nseg, ch);
-          const float b = self_edge ? __ldg(a.selfv + fn) : horner7(cf, t), h = horner7(ch, t) * inv_r;
+          float cf[kNCoef];
+          load_coef(a.tabf, fn, seg, nsegf, cf);  // function-major: row fn, column seg
+          float p, dp;
+          horner7_d(cf, t, p, dp);
+          const float b = self_edge ? __ldg(a.selfv + fn) : p, h = dp * dt_r;
           const float* gr = gs + n * KC + l * l;
 #pragma unroll
           for (int m = 0; m < 2 * l + 1; ++m) {
@@ -339,7 +483,13 @@ struct ForceDispatch {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     // G = dE/dc
     const int SN = a.S * a.N;
-    const int64_t dense_bytes = 4 * (int64_t)(((SN * ((L + 1) * (L + 1) | 1) + 3) & ~3) + (L + 1) * SN * (SN + 1));
+    constexpr int K = (L + 1) * (L + 1);
+    // the pipelined dense kernel: W indices must fit 16 bits, shared memory 200 KB
+    const bool aligned = ((uintptr_t)a.dEdp % 16 == 0) && ((uintptr_t)a.coeff % 16 == 0) && a.F % 4 == 0 &&
+                         (SN * K) % 4 == 0;
+    const int64_t pipe_bulk = 4 * (int64_t)g_layout<L>(a.F, SN, 2).total;
+    const int64_t pipe_plain = 4 * (int64_t)g_layout<L>(a.F, SN, 1).total;
+    const bool pipe_ok = (int64_t)(L + 1) * SN * (SN + 1) < 65536 && pipe_plain <= 200 * 1024;
     if (out_mode == SOAPB_OUT_CC) {
       const int64_t n = a.n_centres * SN * (L + 1) * (L + 1);
       int64_t blocks = (n + 255) / 256;
@@ -347,9 +497,10 @@ struct ForceDispatch {
       k_adjoint_g_cc<<<(unsigned)blocks, 256, 0, st>>>(a, (L + 1) * (L + 1));
       int rc = check_launch("k_adjoint_g_cc");
       if (rc) return rc;
-    } else if (dense_bytes <= 100 * 1024) {
-      auto kern = k_adjoint_g_dense<L>;
-      const int smem = (int)dense_bytes;
+    } else if (pipe_ok) {
+      const bool bulk = aligned && pipe_bulk <= 200 * 1024;
+      auto kern = bulk ? k_adjoint_g_pipe<L, true> : k_adjoint_g_pipe<L, false>;
+      const int smem = (int)(bulk ? pipe_bulk : pipe_plain);
       int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                           "adjoint smem attribute");
       if (rc) return rc;
@@ -358,7 +509,7 @@ struct ForceDispatch {
       int64_t blocks = (int64_t)nsm * occ;
       if (blocks > a.n_centres) blocks = a.n_centres;
       kern<<<(unsigned)blocks, kGThreads, smem, st>>>(a);
-      if ((rc = check_launch("k_adjoint_g_dense"))) return rc;
+      if ((rc = check_launch("k_adjoint_g_pipe"))) return rc;
     } else {
       const int cbytes = 4 * ((a.S * a.N * ((L + 1) * (L + 1) | 1) + 3) & ~3);
       const bool stage = cbytes + 4 * (int64_t)a.F <= 100 * 1024;
@@ -433,8 +584,7 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.coeff = d_coeff;
   a.dEdp = d_dEdp;
   a.centre_atom = d_centre_atom;
-  a.tabt_b = (const float*)((const char*)b->dev + b->off_tabt_b);
-  a.tabt_bh = (const float*)((const char*)b->dev + b->off_tabt_bh);
+  a.tabf = (const float*)((const char*)b->dev + b->off_tabf);
   a.selfv = (const float*)((const char*)b->dev + b->off_self);
   a.widx = (const int*)((const char*)b->dev + b->off_widx);
   a.ftab = (const int*)((const char*)b->dev + b->off_ftab);
@@ -444,11 +594,11 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.n_centres = n_centres;
   a.N = b->n_max;
   a.S = b->n_species;
-  a.nseg = b->n_seg;
+  a.nsegf = 2 * b->n_seg;
   a.F = b->n_feat_ps;
   a.attach = attach ? 1 : 0;
   a.crossover = b->crossover ? 1 : 0;
-  a.inv_h = (float)(1.0 / b->seg_width);
+  a.inv_hf = (float)(2.0 / b->seg_width);
   int rc = check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st), "reset work counter");
   if (rc) return rc;
   return dispatch_l<ForceDispatch>(b->l_max, a, b->tune[2], (int)out_mode, st);

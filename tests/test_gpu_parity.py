@@ -307,6 +307,30 @@ def test_forces_many_species_vs_oracle():
     assert rel_l2(-pt.grad.cpu().numpy(), Fo) < DERIV_TOL
 
 
+@pytest.mark.parametrize("n_max,l_max", [(3, 2), (5, 4)])
+def test_forces_unaligned_rows_vs_oracle(n_max, l_max):
+    """Feature counts F = 63 and 275 and coefficient rows of 54 and 250 floats
+    are not multiples of 4: the G kernel loads its rows with plain loads
+    instead of TMA bulk copies; forces of E = sum w . p against the oracle."""
+    from cusoap_b200 import SOAP
+    rng = np.random.default_rng(12)
+    n = 40
+    pos = rng.uniform(0.0, 7.0, size=(n, 3))
+    Z = rng.choice([1, 8], size=n)
+    P = dict(species=[1, 8], r_cut=4.0, n_max=n_max, l_max=l_max, sigma=0.5)
+    s = SOAP(**P)
+    o = OracleSOAP(**P)
+    F = s.get_number_of_features()
+    assert F % 4 != 0
+    w = rng.standard_normal(F)
+    pt = torch.tensor(pos, device="cuda", requires_grad=True)
+    E = (s.create({"positions": pt, "atomic_numbers": Z}) * torch.tensor(w, dtype=torch.float32,
+                                                                         device="cuda")).sum()
+    E.backward()
+    Fo = o.forces(pos, Z, np.tile(w, (n, 1)))
+    assert rel_l2(-pt.grad.cpu().numpy(), Fo) < DERIV_TOL
+
+
 @pytest.mark.parametrize("name", ["cluster192", "waterbox2001"])
 def test_forces_cc_vs_oracle(name):
     """average='cc' is differentiable too: the adjoint runs the cc layout's
