@@ -43,7 +43,6 @@ struct ForceArgs {
   const float* dEdp;
   const int* centre_atom;
   const float* tabf;     // [fn][nsegf][8]: w B on half-width segments; its derivative is D = d(w B)/dr
-  const float* selfv;    // w0 B_nl(0) for r = 0 edges
   const int* widx;
   const int* ftab;       // l-major pair indices of every feature
   float* G;              // (n_centres, S N K) workspace
@@ -396,7 +395,9 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
           load_coef(a.tabf, fn, seg, nsegf, cf);  // function-major: row fn, column seg
           float p, dp;
           horner7_d(cf, t, p, dp);
-          const float b = self_edge ? __ldg(a.selfv + fn) : p, h = dp * dt_r;
+          // an r = 0 edge adds nothing: its l = 0 term has no gradient and
+          // B_nl(0) = 0 for l >= 1, so b = 0 there (and h = 0 through dt_r)
+          const float b = self_edge ? 0.0f : p, h = dp * dt_r;
           const float* gr = gs + n * KC + l * l;
 #pragma unroll
           for (int m = 0; m < 2 * l + 1; ++m) {
@@ -585,7 +586,6 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.dEdp = d_dEdp;
   a.centre_atom = d_centre_atom;
   a.tabf = (const float*)((const char*)b->dev + b->off_tabf);
-  a.selfv = (const float*)((const char*)b->dev + b->off_self);
   a.widx = (const int*)((const char*)b->dev + b->off_widx);
   a.ftab = (const int*)((const char*)b->dev + b->off_ftab);
   a.G = (float*)d_work;
