@@ -29,7 +29,8 @@ struct GridDesc {
   double fmin[3];  // bin origin in fractional coordinates (non-periodic axes)
   double binw[3];  // fractional bin width
   int nb[3], win[3], nrep[3], per[3];
-  int any_per, pad;
+  int any_per;
+  int orth;  // diagonal frame (every non-periodic structure, rectangular cells): sphere-trimmed enumeration
 };
 
 struct NLWork {
@@ -237,7 +238,9 @@ __global__ void k_grid_init(soapb_structs s, NLWork w, double cutoff) {
     g.nrep[k] = 0;
   }
   g.any_per = anyp;
-  g.pad = 0;
+  g.orth = 1;
+  for (int k = 0; k < 9; ++k)
+    if (k % 4 == 0 ? !(H[k] > 0.0) : H[k] != 0.0) g.orth = 0;
   // perpendicular widths |det| / |cross of the other two rows| (SG:369-379)
   double perp[3];
   for (int k = 0; k < 3; ++k) {
@@ -312,9 +315,14 @@ __global__ void k_grid_setup(soapb_structs s, NLWork w, double cutoff) {
     perp[k] = det / (sqrt(cx * cx + cy * cy + cz * cz) + 1e-300);
   }
   const int64_t A = s.d_atom_off[i + 1] - s.d_atom_off[i];
-  // bins of perpendicular width >= cutoff / 2 (a +-2 bin window): 5^3 half-width
-  // bins hold 15.6 cutoff^3 of candidates against 27 cutoff^3 for full-width bins
-  const double bin_min = 0.5 * cutoff;
+  // Diagonal frames: bins of width >= cutoff / 4, each window row trimmed to
+  // the cutoff sphere (visit_fine), unless a periodic x axis would get fewer
+  // than 3 bins (a row of the window would wrap into more than 4 runs).
+  // Other frames: bins of perpendicular width >= cutoff / 2 and the full
+  // +-2 window: 5^3 half-width bins hold 15.6 cutoff^3 of candidates against
+  // 27 cutoff^3 for full-width bins.
+  if (g.orth && g.per[0] && perp[0] < 0.75 * cutoff) g.orth = 0;
+  const double bin_min = (g.orth ? 0.25 : 0.5) * cutoff;
   for (int k = 0; k < 3; ++k) {
     if (g.per[k]) {
       const int nb = (int)floor(perp[k] / bin_min);
@@ -341,6 +349,7 @@ __global__ void k_grid_setup(soapb_structs s, NLWork w, double cutoff) {
     g.nb[k] = max(1, g.nb[k] / 2);
     g.binw[k] = span / g.nb[k];
   }
+  if (g.orth && g.per[0] && g.nb[0] < 3) g.orth = 0;
   for (int k = 0; k < 3; ++k) {
     const double bw_perp = g.binw[k] * perp[k];  // perpendicular width of one bin
     int win = (int)ceil(cutoff / bw_perp);
@@ -459,7 +468,8 @@ struct VisitArgs {
   const double4* sorted_pos;
   const double4* cpos;
   const int4* cinfo;
-  double cutoff2;
+  int* status;
+  double cutoff, cutoff2;
   int mode;
 };
 
@@ -534,12 +544,175 @@ __device__ __forceinline__ void visit(const VisitArgs& A, int64_t c, Fn&& fn) {
   }
 }
 
+// Sphere-trimmed enumeration for diagonal frames (x = f diag(L)): the rows
+// (bz, by) of unwrapped bins whose slab comes within the cutoff of the
+// centre, each trimmed to the bins x that the sphere's cross-section reaches
+// (conservatively: the cutoff plus 1e-8 A).  Up to 32 rows are laid out at a
+// time, one per lane; a row's x bins are at most 4 runs of contiguous
+// bin-sorted atoms (periodic x axes have >= 3 bins).  The runs of the 32 rows
+// form one candidate stream that all lanes walk 32 at a time: a lane finds
+// its run from the run starts inside its tile (one OR-reduction and a
+// popcount).  Candidate order: z rows, then y, then x, then atom index --
+// deterministic, like the full window's.
+constexpr int kRunsPerPass = 128;  // 32 rows x at most 4 runs
+
+template <class Fn>
+__device__ __forceinline__ void visit_fine(const VisitArgs& A, int64_t c, int* runs, Fn&& fn) {
+  const int lane = threadIdx.x & 31;
+  const double4 cp = A.cpos[c];
+  const int4 ci = A.cinfo[c];
+  const GridDesc& g = A.grids[ci.y];
+  int cw[3];
+  unpack3(ci.z, cw);
+  const int64_t boff = A.bin_off[ci.y];
+  const double cm = A.cutoff + 1e-8;
+  const double Lv[3] = {g.H[0], g.H[4], g.H[8]};
+  const double cv[3] = {cp.x, cp.y, cp.z};
+  // unwrapped bins of axis k that meet [x0, x1] (clamped to the grid on open axes)
+  auto brange = [&](int k, double x0, double x1, int& lo, int& hi) {
+    double u0 = (x0 / Lv[k] - g.fmin[k]) / g.binw[k], u1 = (x1 / Lv[k] - g.fmin[k]) / g.binw[k];
+    if (!g.per[k]) {
+      u0 = fmin(fmax(u0, -1.0), (double)g.nb[k]);
+      u1 = fmin(fmax(u1, -1.0), (double)g.nb[k]);
+    }
+    lo = (int)floor(u0);
+    hi = (int)floor(u1);
+    if (!g.per[k]) {
+      lo = max(lo, 0);
+      hi = min(hi, g.nb[k] - 1);
+    }
+  };
+  // distance from the centre to the slab of unwrapped bin b on axis k
+  auto dmin = [&](int k, int b) {
+    const double lo = (g.fmin[k] + b * g.binw[k]) * Lv[k], hi = (g.fmin[k] + (b + 1) * g.binw[k]) * Lv[k];
+    return fmax(0.0, fmax(lo - cv[k], cv[k] - hi));
+  };
+  int bz0, bz1, by0, by1;
+  brange(2, cp.z - cm, cp.z + cm, bz0, bz1);
+  brange(1, cp.y - cm, cp.y + cm, by0, by1);
+  const int ny = by1 - by0 + 1, nz = bz1 - bz0 + 1;
+  const int nrows = (ny > 0 && nz > 0) ? ny * nz : 0;
+  int* r_start = runs;
+  int* r_s0 = runs + kRunsPerPass;
+  int* r_T = runs + 2 * kRunsPerPass;
+  for (int p0 = 0; p0 < nrows; p0 += 32) {
+    // this lane's row and its x runs (slots with len 0 are unused)
+    const int row = p0 + lane;
+    int rs0[4], rlen[4], rT[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) { rs0[q] = 0; rlen[q] = 0; rT[q] = 0; }
+    if (row < nrows) {
+      const int bz = bz0 + row / ny, by = by0 + row % ny;
+      const double dy = dmin(1, by), dz = dmin(2, bz), d2 = dy * dy + dz * dz;
+      if (d2 <= cm * cm) {
+        const double ext = sqrt(cm * cm - d2);
+        int bx0, bx1;
+        brange(0, cp.x - ext, cp.x + ext, bx0, bx1);
+        int Ty = 0, byw = by, Tz = 0, bzw = bz;
+        if (g.per[1]) { Ty = floordiv(by, g.nb[1]); byw = by - Ty * g.nb[1]; }
+        if (g.per[2]) { Tz = floordiv(bz, g.nb[2]); bzw = bz - Tz * g.nb[2]; }
+        const int64_t gb = boff + ((int64_t)bzw * g.nb[1] + byw) * g.nb[0];
+        int bx = bx0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (bx <= bx1) {
+            int Tx = 0, lx = bx, rend = bx1;
+            if (g.per[0]) {
+              Tx = floordiv(bx, g.nb[0]);
+              lx = bx - Tx * g.nb[0];
+              rend = min(bx1, bx + (g.nb[0] - 1 - lx));
+            }
+            const int64_t s0 = A.bin_start[gb + lx], s1 = A.bin_start[gb + lx + (rend - bx) + 1];
+            rs0[q] = (int)s0;
+            rlen[q] = (int)(s1 - s0);
+            rT[q] = pack3(Tx, Ty, Tz);
+            bx = rend + 1;
+          }
+        }
+        if (bx <= bx1) atomicOr(A.status, 8);  // more than 4 runs: cannot happen with >= 3 bins on x
+      }
+    }
+    int nr = 0, cnt = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      nr += rlen[q] > 0;
+      cnt += rlen[q];
+    }
+    int nr_inc = nr, cnt_inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int a = __shfl_up_sync(0xffffffffu, nr_inc, o), b = __shfl_up_sync(0xffffffffu, cnt_inc, o);
+      if (lane >= o) {
+        nr_inc += a;
+        cnt_inc += b;
+      }
+    }
+    const int nruns = __shfl_sync(0xffffffffu, nr_inc, 31), total = __shfl_sync(0xffffffffu, cnt_inc, 31);
+    {
+      int slot = nr_inc - nr, start = cnt_inc - cnt;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (rlen[q] > 0) {
+          r_start[slot] = start;
+          r_s0[slot] = rs0[q];
+          r_T[slot] = rT[q];
+          start += rlen[q];
+          ++slot;
+        }
+    }
+    __syncwarp();
+    int rb = -1;  // run of the position before the tile
+    for (int k0 = 0; k0 < total; k0 += 32) {
+      const int idx = rb + 1 + lane;
+      const int pos = (idx < nruns) ? r_start[idx] - k0 : 32;
+      const unsigned mask = __reduce_or_sync(0xffffffffu, (pos >= 0 && pos < 32) ? (1u << pos) : 0u);
+      const int run = rb + __popc(mask & ((2u << lane) - 1u));
+      rb = __shfl_sync(0xffffffffu, run, 31);
+      const int k = k0 + lane;
+      bool ok = false;
+      int atom = 0, sp = 0;
+      double rx = 0.0, ry = 0.0, rz = 0.0, r2 = 0.0;
+      if (k < total) {
+        int T[3];
+        unpack3(r_T[run], T);
+        const double4 p = A.sorted_pos[(int64_t)r_s0[run] + (k - r_start[run])];
+        int wrap;
+        unpack_info(p.w, atom, sp, wrap);
+        rx = p.x + (T[0] * Lv[0] - cp.x);
+        ry = p.y + (T[1] * Lv[1] - cp.y);
+        rz = p.z + (T[2] * Lv[2] - cp.z);
+        r2 = rx * rx + ry * ry + rz * rz;
+        ok = r2 <= A.cutoff2;
+        if (ok && g.any_per) {
+          int aw[3];
+          unpack3(wrap, aw);
+#pragma unroll
+          for (int kk = 0; kk < 3; ++kk)
+            if (g.per[kk]) ok &= abs(T[kk] - aw[kk] + cw[kk]) <= g.nrep[kk];
+        }
+        if (ok && A.mode == SOAPB_NL_CREATE && r2 <= 1e-24 && atom != ci.w) ok = false;
+      }
+      fn(ok, atom, sp, rx, ry, rz, r2);
+    }
+    __syncwarp();  // the next pass rewrites the run table
+  }
+}
+
+// The enumeration for the centre's structure: sphere-trimmed for diagonal
+// frames, the full window otherwise (runs: kRunsPerPass * 3 ints of the warp's shared memory).
+template <class Fn>
+__device__ __forceinline__ void visit_any(const VisitArgs& A, int64_t c, int* runs, Fn&& fn) {
+  if (A.grids[A.cinfo[c].y].orth) visit_fine(A, c, runs, fn);
+  else visit(A, c, fn);
+}
+
 __global__ void __launch_bounds__(128) k_count(VisitArgs A, int64_t n_centres, int* counts) {
+  __shared__ int s_runs[4][3 * kRunsPerPass];
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < n_centres; c += nw) {
     int cnt = 0;
-    visit(A, c, [&](bool ok, int, int, double, double, double, double) {
+    visit_any(A, c, s_runs[threadIdx.x >> 5], [&](bool ok, int, int, double, double, double, double) {
       cnt += __popc(__ballot_sync(0xffffffffu, ok));
     });
     if (lane == 0) counts[c] = cnt;
@@ -563,6 +736,8 @@ __global__ void __launch_bounds__(128) k_fill(VisitArgs A, int64_t n_centres, co
               (size_t)wid * kFillStage;
   int* hist = reinterpret_cast<int*>(reinterpret_cast<float4*>(s_raw) + (size_t)(blockDim.x >> 5) * kFillStage) +
               (size_t)(blockDim.x >> 5) * kFillStage + (size_t)wid * nkeys;
+  int* runs = reinterpret_cast<int*>(reinterpret_cast<float4*>(s_raw) + (size_t)(blockDim.x >> 5) * kFillStage) +
+              (size_t)(blockDim.x >> 5) * (kFillStage + nkeys) + (size_t)wid * 3 * kRunsPerPass;
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
   if (pair_off[n_centres] > capacity) {
     if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(status, 4);
@@ -598,7 +773,7 @@ __global__ void __launch_bounds__(128) k_fill(VisitArgs A, int64_t n_centres, co
     __syncwarp();
     if (P <= kFillStage) {
       int n = 0;
-      visit(A, c, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double r2) {
+      visit_any(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double r2) {
         const unsigned bal = __ballot_sync(0xffffffffu, ok);
         if (ok) {
           const int pos = n + __popc(bal & ((1u << lane) - 1u));
@@ -629,12 +804,12 @@ __global__ void __launch_bounds__(128) k_fill(VisitArgs A, int64_t n_centres, co
         __syncwarp();
       }
     } else {
-      visit(A, c, [&](bool ok, int, int sp, double, double, double, double r2) {
+      visit_any(A, c, runs, [&](bool ok, int, int sp, double, double, double, double r2) {
         if (ok) atomicAdd(&hist[keyof(sp, r2)], 1);
       });
       __syncwarp();
       scan_hist();
-      visit(A, c, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double r2) {
+      visit_any(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double r2) {
         const int key = ok ? keyof(sp, r2) : -1 - lane;
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         const int rank = __popc(peers & ((1u << lane) - 1u));
@@ -768,6 +943,8 @@ static VisitArgs visit_args(const soapb_basis* b, const NLWork& w, int mode) {
   A.sorted_pos = w.sorted_pos;
   A.cpos = w.cpos;
   A.cinfo = w.cinfo;
+  A.status = w.status;
+  A.cutoff = b->cutoff;
   A.cutoff2 = b->cutoff * b->cutoff;
   A.mode = mode;
   return A;
@@ -842,7 +1019,7 @@ extern "C" int soapb_neighbors_fill(const soapb_basis* b, const soapb_structs* s
   NLWork w = nl_work(L, d_work);
   const VisitArgs A = visit_args(b, w, mode);
   if (c->n_centres > 0) {
-    const int smem = 4 * (16 * kFillStage + 4 * kFillStage + 4 * b->n_keys);
+    const int smem = 4 * (16 * kFillStage + 4 * kFillStage + 4 * b->n_keys + 4 * 3 * kRunsPerPass);
     int rc2 = check_cuda(cudaFuncSetAttribute(k_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                          "fill smem attribute");
     if (rc2) return rc2;

@@ -209,6 +209,8 @@ class _Pairs:
             raise ValueError("singular cell in a periodic structure")
         if status & 2:
             raise ValueError("an atom lies more than 511 cells outside its periodic cell")
+        if status & 8:
+            raise RuntimeError("neighbour enumeration: a window row exceeded its run limit")
         if status:
             raise _lib.SoapbError(_lib.ERR_CAPACITY, f"neighbour list status {status}")
         # the list is allocated to the exact total, so the fill cannot overflow it

@@ -162,7 +162,9 @@ int soapb_neighbors_fill(const soapb_basis* b, const soapb_structs* s, const soa
                          int64_t capacity, void* stream);
 /* Error flags of the last count/fill on this workspace (synchronises the
  * stream): bit 0 singular cell, bit 1 atom more than 511 cells outside its
- * cell, bit 2 pair capacity exceeded.  0 = no error. */
+ * cell, bit 2 pair capacity exceeded, bit 3 internal enumeration limit (a
+ * window row of more than 4 runs; not reachable by construction).  0 = no
+ * error. */
 int soapb_neighbors_status(const soapb_basis* b, const soapb_structs* s, const soapb_centres* c, void* d_work,
                            int32_t* h_status, void* stream);
 
