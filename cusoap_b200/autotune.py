@@ -7,7 +7,7 @@ system and keeps the fastest:
 * descriptor: warps per block (1, 2, 4) x radial functions per lane (the
   minimum for n_max and l_max, and the next supported size above it: more
   functions per lane means fewer busy lanes but more independent work per
-  lane);
+  lane; with two pair streams per warp only the warps per block);
 * adjoint edge kernel: warps per block (1, 2, 4).
 
 The choice is written into the basis (``soapb_basis.tune``), so every later
@@ -37,8 +37,24 @@ def min_functions_per_lane(n_max: int, l_max: int) -> int:
     return 6 if gn == 5 else gn
 
 
+def two_pair_streams(n_max: int, l_max: int) -> bool:
+    """The descriptor kernel's lane map for (n_max, l_max) -- the rule of
+    desc_two_streams in csrc/descriptor.cu: two pair streams per warp (its
+    functions per lane fixed) for l_max <= 4 when one stream would leave more
+    than a quarter of the lanes without a radial function."""
+    if l_max > 4:
+        return False
+    lpl = 16 // (l_max + 1)
+    if -(-n_max // lpl) > 3:
+        return False
+    gn = min_functions_per_lane(n_max, l_max)
+    return (l_max + 1) * -(-n_max // gn) <= 24
+
+
 def descriptor_candidates(n_max: int, l_max: int) -> List[Tuple[int, int]]:
     g0 = min_functions_per_lane(n_max, l_max)
+    if two_pair_streams(n_max, l_max):  # functions per lane are not a choice there
+        return [(w, g0) for w in (1, 2, 4)]
     gns = [g for g in _GN_SIZES if g >= g0][:2]
     return [(w, g) for w in (1, 2, 4) for g in gns]
 

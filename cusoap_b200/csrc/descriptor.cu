@@ -58,22 +58,63 @@ constexpr bool ybase_banks_distinct() {
 }
 static_assert(ybase_banks_distinct(), "Y row blocks must start on distinct banks");
 
+// Extra offset of the Y rows of pairs 16..31 (two pair streams per warp): the
+// smallest shift that keeps the l blocks of row q and row q + 16 -- read by
+// the two half-warps at once -- on distinct banks.
+__host__ __device__ constexpr int half_offset(int L, int YS) {
+  for (int h = 0; h < 32; ++h) {
+    bool ok = true;
+    for (int l = 0; l <= L; ++l)
+      for (int k = 0; k <= L; ++k)
+        if ((16 * YS + h + ybase(l)) % 32 == ybase(k) % 32) ok = false;
+    if (ok) return h;
+  }
+  return 0;
+}
+
 template <int L>
 struct DescShape {
   static constexpr int K = (L + 1) * (L + 1);
   static constexpr int YS = (ybase(L) + 2 * L + 1) | 1;  // odd strides: conflict-free row writes
+  static constexpr int HOFF = half_offset(L, YS);
   static constexpr int KC = K | 1;
-  __host__ __device__ static int warp_floats(int S, int N) { return 32 * YS + 96 + S * N * KC; }
+  __host__ __device__ static int warp_floats(int S, int N) { return 32 * YS + HOFF + 96 + S * N * KC; }
 };
+
+// Functions per lane for (N, L): floor(32 / (L+1)) lanes share each l.
+inline int desc_group(int N, int L) {
+  const int lpl = 32 / (L + 1);
+  int gn = (N + lpl - 1) / lpl;
+  if (gn == 5) gn = 6;
+  return gn;
+}
+
+// Two pair streams per warp (each half-warp walks 16 of every 32 pairs, lanes
+// grouped by l inside the half, at most 3 functions per lane), for l_max <= 4
+// when one stream leaves more than a quarter of the lanes without a function
+// (n_max 8, l_max 4: 20 of 32 lanes busy with one stream, 30 with two).
+inline bool desc_two_streams(int N, int L) {
+  if (L > 4) return false;
+  const int lpl = 16 / (L + 1);
+  if ((N + lpl - 1) / lpl > 3) return false;
+  const int gn = desc_group(N, L);
+  return (L + 1) * ((N + gn - 1) / gn) <= 24;
+}
 
 constexpr int kMaxBlocks = kMaxS * (kMaxS + 1) / 2;
 constexpr int kMaxTri = kMaxN * (kMaxN + 1) / 2;
 
-template <int L, int GN>
-__global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
+// H pair streams per warp (1, or 2 for small l_max): half-warp h takes pairs
+// 16 h .. 16 h + 15 of every staged batch of 32.  Each stream keeps its own
+// species and segment; the streams flush their species partials into the
+// centre's coefficient buffer one after the other, so sums are deterministic.
+template <int L, int GN, int H>
+__device__ __forceinline__ void descriptor_body(const DescArgs& a) {
   using Sh = DescShape<L>;
   constexpr int K = Sh::K, YS = Sh::YS, KC = Sh::KC, M = 2 * L + 1;
-  constexpr int LPL = 32 / (L + 1);  // lanes per l
+  constexpr int HL = 32 / H;           // lanes per stream
+  constexpr int LPL = HL / (L + 1);    // lanes per l
+  constexpr int HOFF = (H == 2) ? Sh::HOFF : 0;
   extern __shared__ float sm[];
   __shared__ float s_pref[kMaxL + 1];
   __shared__ int s_blk[2 * kMaxBlocks];              // (j | jd << 8, first feature) per species block
@@ -82,7 +123,7 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
   const int N = a.N, S = a.S, NF = N * (L + 1);
   const int cbn = S * N * KC;
   float* Y = sm + (size_t)wid * Sh::warp_floats(S, N);
-  float* tt = Y + 32 * YS;
+  float* tt = Y + 32 * YS + Sh::HOFF;
   int* sg = (int*)(tt + 32);
   int* spp = sg + 32;
   float* cbuf = (float*)(spp + 32);
@@ -107,12 +148,13 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
   const int nblk = a.crossover ? S * (S + 1) / 2 : S;
   const int q32 = 32 / N, r32 = 32 % N;  // p -> p + 32 in the off-diagonal (n, n') order
 
-  // lane -> l and its functions n = k GN + g
-  const int l_me = lane / LPL, k_me = lane % LPL;
+  // lane -> stream, l and its functions n = k GN + g
+  const int h = (H == 2) ? (lane >> 4) : 0, hl = lane & (HL - 1);
+  const int l_me = hl / LPL, k_me = hl % LPL;
   const bool active = l_me <= L && k_me * GN < N;
   const int lme = active ? l_me : 0;
   const int mme = 2 * lme + 1;
-  const int ybm = ybase(lme);
+  const int ybm = ybase(lme) + h * (16 * YS + HOFF);  // this stream's row block
   float selfb[GN];
 #pragma unroll
   for (int g = 0; g < GN; ++g) {
@@ -171,17 +213,29 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
         tt[lane] = (r > 0.0f) ? t : 3.0f;  // 3: r = 0 edge, takes the self value
         sg[lane] = seg;
         spp[lane] = (int)((unsigned)w >> kAtomBits);
-        float* yrow = Y + lane * YS;
+        float* yrow = Y + lane * YS + ((H == 2 && lane >= 16) ? HOFF : 0);
         SolidHarmonics<L>::values(pr.x, pr.y, pr.z, [&](int idx, float v) { yrow[ypos(idx)] = v; });
       }
       __syncwarp();
-      for (int q = 0; q < nt; ++q) {
-        const int sp = spp[q];
-        if (sp != cur_sp) {
-          if (cur_sp >= 0) flush(cur_sp);
+      const int nq = (H == 2) ? min(nt, 16) : nt;
+      for (int j = 0; j < nq; ++j) {
+        const int q = h * 16 + j;
+        const bool valid = (H == 1) || q < nt;  // the second stream of a short batch idles
+        const int sp = valid ? spp[q] : cur_sp;
+        if (H == 1) {
+          if (sp != cur_sp) {
+            if (cur_sp >= 0) flush(cur_sp);
+            cur_sp = sp;
+          }
+        } else if (__any_sync(0xffffffffu, sp != cur_sp)) {
+#pragma unroll
+          for (int hh = 0; hh < H; ++hh) {  // stream 0 first, then stream 1
+            if (h == hh && sp != cur_sp && cur_sp >= 0) flush(cur_sp);
+            __syncwarp();
+          }
           cur_sp = sp;
         }
-        const int seg = sg[q];
+        const int seg = valid ? sg[q] : cur_seg;
         if (seg != cur_seg) {
           if (active) {
 #pragma unroll
@@ -192,25 +246,30 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
           }
           cur_seg = seg;
         }
-        const float t = tt[q];
-        float B[GN];
+        if (valid) {
+          const float t = tt[q];
+          float B[GN];
 #pragma unroll
-        for (int g = 0; g < GN; ++g) B[g] = (t > 2.0f) ? selfb[g] : horner7(cf[g], t);
-        // all M slots, without a per-lane test: slots m >= 2l+1 read on along
-        // the row (position <= ybase(l) + 2L < YS, in bounds) and collect
-        // values that flush() never stores, so no branch is needed per slot
-        const float* yr = Y + q * YS + ybm;
+          for (int g = 0; g < GN; ++g) B[g] = (t > 2.0f) ? selfb[g] : horner7(cf[g], t);
+          // all M slots, without a per-lane test: slots m >= 2l+1 read on along
+          // the row (position <= ybase(l) + 2L < YS, in bounds) and collect
+          // values that flush() never stores, so no branch is needed per slot
+          const float* yr = Y + j * YS + ybm;
 #pragma unroll
-        for (int m = 0; m < M; ++m) {
-          const float yv = yr[m];
+          for (int m = 0; m < M; ++m) {
+            const float yv = yr[m];
 #pragma unroll
-          for (int g = 0; g < GN; ++g) acc[g][m] = fmaf(B[g], yv, acc[g][m]);
+            for (int g = 0; g < GN; ++g) acc[g][m] = fmaf(B[g], yv, acc[g][m]);
+          }
         }
       }
       __syncwarp();
     }
-    if (cur_sp >= 0) flush(cur_sp);
-    __syncwarp();
+#pragma unroll
+    for (int hh = 0; hh < H; ++hh) {
+      if (h == hh && cur_sp >= 0) flush(cur_sp);
+      __syncwarp();
+    }
 
     if (a.coeff_out) {
       float* crow = a.coeff_out + (size_t)c * S * N * K;
@@ -268,15 +327,18 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
   }
 }
 
-// Functions per lane for (N, L): floor(32 / (L+1)) lanes share each l.
-inline int desc_group(int N, int L) {
-  const int lpl = 32 / (L + 1);
-  int gn = (N + lpl - 1) / lpl;
-  if (gn == 5) gn = 6;
-  return gn;
+template <int L, int GN>
+__global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
+  descriptor_body<L, GN, 1>(a);
 }
 
+// Two pair streams (l_max <= 4): registers capped for 5 blocks of 4 warps per SM.
 template <int L, int GN>
+__global__ void __launch_bounds__(128, 5) k_descriptor_2s(DescArgs a) {
+  descriptor_body<L, GN, 2>(a);
+}
+
+template <int L, int GN, int H>
 static int launch_descriptor(const DescArgs& a, int wpb_tuned, cudaStream_t st) {
   const int per_warp = 4 * DescShape<L>::warp_floats(a.S, a.N);
   int wpb = (200 * 1024) / per_warp;
@@ -284,7 +346,7 @@ static int launch_descriptor(const DescArgs& a, int wpb_tuned, cudaStream_t st) 
   if ((wpb_tuned == 1 || wpb_tuned == 2 || wpb_tuned == 4) && wpb_tuned <= wpb) wpb = wpb_tuned;
   if (wpb < 1) return set_error(SOAPB_ERR_UNSUPPORTED, "descriptor shared memory %d B per warp too large", per_warp);
   const int smem = wpb * per_warp;
-  auto kern = k_descriptor<L, GN>;
+  auto kern = (H == 2) ? k_descriptor_2s<L, GN> : k_descriptor<L, GN>;
   int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                       "descriptor smem attribute");
   if (rc) return rc;
@@ -304,12 +366,22 @@ static int launch_descriptor(const DescArgs& a, int wpb_tuned, cudaStream_t st) 
 template <int L>
 struct DescDispatch {
   static int run(const DescArgs& a, int gn, int wpb, cudaStream_t st) {
+    if constexpr (L <= 4) {
+      if (desc_two_streams(a.N, L)) {  // functions per lane fixed by (N, L): ceil(N / floor(16 / (L+1)))
+        const int lpl = 16 / (L + 1), g2 = (a.N + lpl - 1) / lpl;
+        switch (g2) {
+          case 1: return launch_descriptor<L, 1, 2>(a, wpb, st);
+          case 2: return launch_descriptor<L, 2, 2>(a, wpb, st);
+          default: return launch_descriptor<L, 3, 2>(a, wpb, st);
+        }
+      }
+    }
     switch (gn) {
-      case 1: return launch_descriptor<L, 1>(a, wpb, st);
-      case 2: return launch_descriptor<L, 2>(a, wpb, st);
-      case 3: return launch_descriptor<L, 3>(a, wpb, st);
-      case 4: return launch_descriptor<L, 4>(a, wpb, st);
-      case 6: return launch_descriptor<L, 6>(a, wpb, st);
+      case 1: return launch_descriptor<L, 1, 1>(a, wpb, st);
+      case 2: return launch_descriptor<L, 2, 1>(a, wpb, st);
+      case 3: return launch_descriptor<L, 3, 1>(a, wpb, st);
+      case 4: return launch_descriptor<L, 4, 1>(a, wpb, st);
+      case 6: return launch_descriptor<L, 6, 1>(a, wpb, st);
       default: return set_error(SOAPB_ERR_UNSUPPORTED, "descriptor: %d radial functions per lane not built", gn);
     }
   }

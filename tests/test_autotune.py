@@ -20,6 +20,20 @@ def test_min_functions_per_lane_covers_every_function():
             assert len(cands) >= 3
 
 
+def test_two_pair_streams_rule():
+    # n_max 8, l_max 4 (the 1M-atom cluster): one stream keeps 20 of 32 lanes busy
+    assert AT.two_pair_streams(8, 4)
+    # n_max 7, l_max 3 (28 lanes busy) and every l_max > 4 keep one stream
+    assert not AT.two_pair_streams(7, 3)
+    assert not AT.two_pair_streams(8, 6)
+    for L in range(5):
+        for N in range(1, 17):
+            if AT.two_pair_streams(N, L):
+                lpl = 16 // (L + 1)
+                assert lpl * 3 >= N  # at most 3 functions per lane in a half-warp
+                assert len(AT.descriptor_candidates(N, L)) == 3
+
+
 def test_cache_roundtrip(tmp_path):
     path = os.path.join(tmp_path, "tune.json")
     table = {"B200|N8|L6|S4|x1|rbf=gto": {"desc_wpb": 2, "desc_gn": 2, "force_wpb": 4}}
