@@ -111,7 +111,9 @@ __global__ void __launch_bounds__(kGThreads) k_adjoint_g(ForceArgs a) {
 //    lanes over a).  Entries without a feature stay zero.
 //  - The coefficient row is repacked with every l block on a float4
 //    boundary, so G[a, lm] = pref_l sum_b W_l[a][b] c[b, lm] runs as equal
-//    tasks (a, quad of 4 m slots), c read as float4 broadcasts.
+//    tasks (rows a and a + SN/2, quad of 4 m slots): each float4 broadcast
+//    of c feeds 8 FMAs (a full-warp 128-bit shared read costs 4 wavefronts,
+//    broadcast or not, so the rows share it).
 //  - G goes through shared memory to coalesced row stores.
 // Coefficient row layout of the G kernel: l block l starts at off(l), a multiple of 4.
 template <int L>
@@ -126,6 +128,14 @@ struct GLayout {
   int idx, w, craw, cp, W, G, total, fa, snka;
 };
 
+// Floats per W_l matrix (SN rows of SN + 1): padded to 16 mod 32, so the two
+// half-warps of a G task group, on quads of neighbouring l, read W rows on
+// different banks.
+__host__ __device__ inline int g_wl(int SN) {
+  const int w = SN * (SN + 1);
+  return w + (48 - w % 32) % 32;
+}
+
 template <int L>
 __host__ __device__ inline GLayout g_layout(int F, int SN, int nbuf) {
   constexpr int K = GRow<L>::K, KP = GRow<L>::KP, KG = K | 1;
@@ -137,7 +147,7 @@ __host__ __device__ inline GLayout g_layout(int F, int SN, int nbuf) {
   g.craw = g.w + nbuf * g.fa;
   g.cp = g.craw + nbuf * g.snka;
   g.W = g.cp + SN * KP;
-  g.G = g.W + (((L + 1) * SN * (SN + 1) + 3) & ~3);
+  g.G = g.W + (((L + 1) * g_wl(SN) + 3) & ~3);
   g.total = g.G + ((SN * KG + 3) & ~3);
   return g;
 }
@@ -190,7 +200,7 @@ __global__ void __launch_bounds__(kGThreads) k_adjoint_g_pipe(ForceArgs a) {
   __shared__ int s_quad[KP / 4];  // l | (first m) << 8 of every float4 quad of the padded row
   __shared__ int s_fail;
   const int tid = threadIdx.x, nth = blockDim.x;
-  const int N = a.N, SN = a.S * N, WS = SN + 1, F = a.F, SNK = SN * K;
+  const int N = a.N, SN = a.S * N, WS = SN + 1, WL = g_wl(SN), F = a.F, SNK = SN * K;
   const GLayout ly = g_layout<L>(F, SN, BULK ? 2 : 1);
   int* s_idx = reinterpret_cast<int*>(sm + ly.idx);
   float* s_cp = sm + ly.cp;
@@ -203,7 +213,7 @@ __global__ void __launch_bounds__(kGThreads) k_adjoint_g_pipe(ForceArgs a) {
     const int code = __ldg(a.ftab + f);
     const int l = code >> 24, base = l * SN;
     const int ia = (code & 0xfff) - base, ib = ((code >> 12) & 0xfff) - base;
-    s_idx[f] = ((base + ia) * WS + ib) | (((base + ib) * WS + ia) << 16);
+    s_idx[f] = (l * WL + ia * WS + ib) | ((l * WL + ib * WS + ia) << 16);
   }
   if (tid <= L) s_pref[tid] = sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * tid + 1.0f));
   for (int lm = tid; lm < K; lm += nth) {
@@ -274,30 +284,45 @@ __global__ void __launch_bounds__(kGThreads) k_adjoint_g_pipe(ForceArgs a) {
       s_cp[bi * KP + s_lmoff[i - bi * K]] = c_row[i];
     }
     __syncthreads();
-    // tasks (a, quad): G[a, l^2 + m0 .. m0 + 3] = pref_l sum_b W_l[a][b] c[b, quad], the
-    // quad read as one float4 (lanes over a share it); padding lanes are not stored
-    for (int t = tid; t < SN * (KP / 4); t += nth) {
-      const int qd = t / SN, ai = t - qd * SN;
+    // tasks (row pair, quad): G[a, l^2 + m0 .. m0 + 3] = pref_l sum_b W_l[a][b] c[b, quad]
+    // for the rows a = ap and ap + SNh; the quad is read as one float4 (lanes over ap share
+    // it) and feeds both rows.  Padding slots and a missing second row are not stored.
+    const int SNh = (SN + 1) >> 1;
+    for (int t = tid; t < SNh * (KP / 4); t += nth) {
+      const int qd = t / SNh, a0 = t - qd * SNh, a1 = a0 + SNh;
+      const bool two = a1 < SN;
       const int info = s_quad[qd], l = info & 255, m0 = info >> 8;
-      const float* Wr = s_W + (l * SN + ai) * WS;
+      const float* W0 = s_W + l * WL + a0 * WS;
+      const float* W1 = s_W + l * WL + (two ? a1 : a0) * WS;
       const float4* cq = reinterpret_cast<const float4*>(s_cp) + qd;
-      float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      float4 g = make_float4(0.0f, 0.0f, 0.0f, 0.0f), h = g;
 #pragma unroll 8
       for (int bi = 0; bi < SN; ++bi) {
-        const float w = Wr[bi];
+        const float w0 = W0[bi], w1 = W1[bi];
         const float4 v = cq[bi * (KP / 4)];
-        g.x = fmaf(w, v.x, g.x);
-        g.y = fmaf(w, v.y, g.y);
-        g.z = fmaf(w, v.z, g.z);
-        g.w = fmaf(w, v.w, g.w);
+        g.x = fmaf(w0, v.x, g.x);
+        g.y = fmaf(w0, v.y, g.y);
+        g.z = fmaf(w0, v.z, g.z);
+        g.w = fmaf(w0, v.w, g.w);
+        h.x = fmaf(w1, v.x, h.x);
+        h.y = fmaf(w1, v.y, h.y);
+        h.z = fmaf(w1, v.z, h.z);
+        h.w = fmaf(w1, v.w, h.w);
       }
       const float p = s_pref[l];
       const int M = 2 * l + 1;
-      float* go = s_G + ai * KG + l * l + m0;
+      float* go = s_G + a0 * KG + l * l + m0;
       go[0] = p * g.x;
       if (m0 + 1 < M) go[1] = p * g.y;
       if (m0 + 2 < M) go[2] = p * g.z;
       if (m0 + 3 < M) go[3] = p * g.w;
+      if (two) {
+        float* g1 = s_G + a1 * KG + l * l + m0;
+        g1[0] = p * h.x;
+        if (m0 + 1 < M) g1[1] = p * h.y;
+        if (m0 + 2 < M) g1[2] = p * h.z;
+        if (m0 + 3 < M) g1[3] = p * h.w;
+      }
     }
     __syncthreads();
     float* grow = a.G + c * SNK;
@@ -490,7 +515,7 @@ struct ForceDispatch {
                          (SN * K) % 4 == 0;
     const int64_t pipe_bulk = 4 * (int64_t)g_layout<L>(a.F, SN, 2).total;
     const int64_t pipe_plain = 4 * (int64_t)g_layout<L>(a.F, SN, 1).total;
-    const bool pipe_ok = (int64_t)(L + 1) * SN * (SN + 1) < 65536 && pipe_plain <= 200 * 1024;
+    const bool pipe_ok = (int64_t)(L + 1) * g_wl(SN) < 65536 && pipe_plain <= 200 * 1024;
     if (out_mode == SOAPB_OUT_CC) {
       const int64_t n = a.n_centres * SN * (L + 1) * (L + 1);
       int64_t blocks = (n + 255) / 256;

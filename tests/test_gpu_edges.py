@@ -85,12 +85,21 @@ def _periodic_case(kind, seed=0):
     elif kind == "tiny_cell":
         cell = np.array([[3.3, 0.0, 0.0], [0.4, 3.1, 0.0], [0.0, 0.6, 3.5]])
         pbc = [True, True, True]
+    elif kind == "rect_x_below":  # x side 4.5 A < 0.75 x the 6.36 A cutoff: the full-window path
+        cell = np.diag([4.5, 7.0, 9.0])
+        pbc = [True, True, True]
+    elif kind == "rect_x_above":  # x side 5.0 A: the sphere-trimmed path with 3 bins on x
+        cell = np.diag([5.0, 7.0, 9.0])
+        pbc = [True, True, True]
+    elif kind == "rect_unwrapped":  # rectangular, atoms spread over several cell images
+        cell = np.diag([8.0, 9.5, 11.0])
+        pbc = [True, True, True]
     else:  # unwrapped: atoms spread over several cell images
         cell = np.array([[8.5, 0.0, 0.0], [0.0, 9.5, 0.0], [1.0, 0.0, 9.0]])
         pbc = [True, True, True]
-    n = 4 if kind == "tiny_cell" else 40
+    n = 4 if kind == "tiny_cell" else (12 if kind.startswith("rect_x") else 40)
     frac = rng.uniform(0.0, 1.0, size=(n, 3))
-    if kind == "unwrapped":
+    if kind in ("unwrapped", "rect_unwrapped"):
         frac += rng.integers(-2, 3, size=(n, 3))
     if kind == "mixed_pbc":
         frac[:, 2] = rng.uniform(0.3, 0.5, size=n)
@@ -99,10 +108,14 @@ def _periodic_case(kind, seed=0):
     return {"positions": pos, "atomic_numbers": Z, "cell": cell, "pbc": pbc}
 
 
-@pytest.mark.parametrize("kind", ["triclinic", "mixed_pbc", "tiny_cell", "unwrapped"])
+@pytest.mark.parametrize("kind", ["triclinic", "mixed_pbc", "tiny_cell", "unwrapped", "rect_x_below",
+                                  "rect_x_above", "rect_unwrapped"])
 def test_periodic_geometries_vs_oracle(kind):
-    """create, the Jacobian and the adjoint forces on periodic geometries the
-    workloads do not cover, against the oracle's brute-force image sums."""
+    """create and the adjoint forces on periodic geometries the workloads do
+    not cover, against the oracle's brute-force image sums.  Rectangular
+    cells take the sphere-trimmed neighbour enumeration unless the periodic x
+    side is under 0.75 cutoff (then the full window): both sides of that
+    threshold are here."""
     from cusoap_b200 import SOAP
     P = dict(species=[1, 8], r_cut=4.5, n_max=4, l_max=3, sigma=0.5, periodic=True)
     s = SOAP(**P)
