@@ -408,7 +408,10 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
       const float dt_r = self_edge ? 0.0f : 2.0f * a.inv_hf / r;  // (dt/dr) / r: Bhat = D / r = dP/dt dt_r
       const EdgeHarmonics<L> eh(x, y, z);
       const float* gs = G + sp * N * KC;
-      float ex = 0.f, ey = 0.f, ez = 0.f;
+      // sum_lm (rvec zeta_lm R_lm + xi_lm grad R_lm), grouped: with u = nrm xi, Phi_m = C_m or S_m,
+      //   P1 = sum u Q_{l-1}^{m+1} Phi_m, Pz = sum u (l+m) Q_{l-1}^m Phi_m, Rz = sum zeta R_lm,
+      //   Tx, Ty = sum m Q_l^m (d Phi_m / dx, dy) u:  dE/drvec = (x (Rz - P1) + Tx, y (Rz - P1) + Ty, z Rz + Pz)
+      float P1 = 0.f, Pz = 0.f, Rz = 0.f, Tx = 0.f, Ty = 0.f;
 #pragma unroll
       for (int l = 0; l <= L; ++l) {
         float xi[2 * L + 1], ze[2 * L + 1];
@@ -431,7 +434,7 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
             ze[m] = fmaf(gv, h, ze[m]);
           }
         }
-        // solid harmonics R_l^m and gradients (index l + m within the l block)
+        // this l's terms of the grouped sums (xi / ze index l + m within the l block)
 #pragma unroll
         for (int m = 0; m <= l; ++m) {
           const float nrm = c_shnorm[l * (kMaxL + 1) + m];
@@ -439,35 +442,25 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
           const float qp = (l >= 1 && m + 1 <= l - 1) ? eh.Q[tri(l - 1, m + 1)] : 0.0f;
           const float qz = (l >= 1 && m <= l - 1) ? (float)(l + m) * eh.Q[tri(l - 1, m)] : 0.0f;
           if (m == 0) {
-            const float R = nrm * q, dx = nrm * (-x * qp), dy = nrm * (-y * qp), dz = nrm * qz;
-            const float zr = ze[l] * R;
-            ex += x * zr + xi[l] * dx;
-            ey += y * zr + xi[l] * dy;
-            ez += z * zr + xi[l] * dz;
+            const float u = nrm * xi[l];
+            P1 = fmaf(u, qp, P1);
+            Pz = fmaf(u, qz, Pz);
+            Rz = fmaf(nrm * q, ze[l], Rz);
           } else {
-            const float fm = (float)m;
             const float Cm = eh.C[m], Sm = eh.Sn[m], Cp = eh.C[m - 1], Sp = eh.Sn[m - 1];
-            {  // +m
-              const float R = nrm * q * Cm;
-              const float dx = nrm * (-x * qp * Cm + q * fm * Cp), dy = nrm * (-y * qp * Cm - q * fm * Sp);
-              const float dz = nrm * qz * Cm;
-              const float zr = ze[l + m] * R;
-              ex += x * zr + xi[l + m] * dx;
-              ey += y * zr + xi[l + m] * dy;
-              ez += z * zr + xi[l + m] * dz;
-            }
-            {  // -m
-              const float R = nrm * q * Sm;
-              const float dx = nrm * (-x * qp * Sm + q * fm * Sp), dy = nrm * (-y * qp * Sm + q * fm * Cp);
-              const float dz = nrm * qz * Sm;
-              const float zr = ze[l - m] * R;
-              ex += x * zr + xi[l - m] * dx;
-              ey += y * zr + xi[l - m] * dy;
-              ez += z * zr + xi[l - m] * dz;
-            }
+            const float u = nrm * xi[l + m], v = nrm * xi[l - m];
+            const float U = fmaf(u, Cm, v * Sm);
+            P1 = fmaf(U, qp, P1);
+            Pz = fmaf(U, qz, Pz);
+            const float mq = (float)m * q;
+            Tx = fmaf(mq, fmaf(u, Cp, v * Sp), Tx);
+            Ty = fmaf(mq, fmaf(v, Cp, -u * Sp), Ty);
+            Rz = fmaf(nrm * q, fmaf(ze[l + m], Cm, ze[l - m] * Sm), Rz);
           }
         }
       }
+      const float rr = Rz - P1;
+      const float ex = fmaf(x, rr, Tx), ey = fmaf(y, rr, Ty), ez = fmaf(z, Rz, Pz);
       if (!(a.attach && atom == catom)) {
         atomicAdd(&a.forces[3 * (size_t)atom + 0], -ex);
         atomicAdd(&a.forces[3 * (size_t)atom + 1], -ey);
