@@ -16,8 +16,8 @@
 // flushes the accumulators into the warp's coefficient buffer, the segment
 // switch (warp-uniform) reloads the lane's table coefficients, so the
 // per-pair work is 7 FMAs of Horner per function plus one FMA per (n, l, m).
-// Solid harmonics are computed 32 pairs at a time, one pair per lane, into
-// shared memory.  The power-spectrum epilogue walks the DScribe blocks
+// Solid harmonics are computed 16 pairs at a time (32 with two pair streams),
+// one pair per lane, into shared memory.  The power-spectrum epilogue walks the DScribe blocks
 // (species pair, l) with the m loop unrolled per l; each lane writes
 // consecutive features, so the row is stored coalesced.
 #include "common.cuh"
@@ -79,6 +79,8 @@ struct DescShape {
   static constexpr int HOFF = half_offset(L, YS);
   static constexpr int KC = K | 1;
   __host__ __device__ static int warp_floats(int S, int N) { return 32 * YS + HOFF + 96 + S * N * KC; }
+  // one pair stream: 16 staged pairs per batch
+  __host__ __device__ static int warp_floats16(int S, int N) { return 16 * YS + 48 + S * N * KC; }
 };
 
 // Functions per lane for (N, L): floor(32 / (L+1)) lanes share each l.
@@ -122,11 +124,14 @@ __device__ __forceinline__ void descriptor_body(const DescArgs& a) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int N = a.N, S = a.S, NF = N * (L + 1);
   const int cbn = S * N * KC;
-  float* Y = sm + (size_t)wid * Sh::warp_floats(S, N);
-  float* tt = Y + 32 * YS + Sh::HOFF;
-  int* sg = (int*)(tt + 32);
-  int* spp = sg + 32;
-  float* cbuf = (float*)(spp + 32);
+  // pairs staged per batch: 16 with one stream (half the harmonic rows in shared
+  // memory, so more warps fit an SM), 32 with two (16 per stream)
+  constexpr int BQ = (H == 2) ? 32 : 16;
+  float* Y = sm + (size_t)wid * ((H == 2) ? Sh::warp_floats(S, N) : Sh::warp_floats16(S, N));
+  float* tt = Y + BQ * YS + ((H == 2) ? Sh::HOFF : 0);
+  int* sg = (int*)(tt + BQ);
+  int* spp = sg + BQ;
+  float* cbuf = (float*)(spp + BQ);
   if (threadIdx.x <= L) s_pref[threadIdx.x] = sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * threadIdx.x + 1.0f));
   if (threadIdx.x == 0) {
     int nb = 0, f = 0;
@@ -201,8 +206,8 @@ __device__ __forceinline__ void descriptor_body(const DescArgs& a) {
         for (int m = 0; m < M; ++m) acc[g][m] = 0.0f;
     };
 
-    for (int64_t base = p0; base < p1; base += 32) {
-      const int nt = (int)min((int64_t)32, p1 - base);
+    for (int64_t base = p0; base < p1; base += BQ) {
+      const int nt = (int)min((int64_t)BQ, p1 - base);
       if (lane < nt) {
         const float4 pr = __ldg(a.pairs + base + lane);
         const int w = __float_as_int(pr.w);
@@ -285,7 +290,7 @@ __device__ __forceinline__ void descriptor_body(const DescArgs& a) {
         const int j = jj & 255, jd = jj >> 8;
         const bool diag = j == jd;
         const int np = diag ? N * (N + 1) / 2 : N * N;
-#pragma unroll
+#pragma unroll 1  // one copy of the l loop: smaller code, fewer instruction-fetch stalls
         for (int l = 0; l <= L; ++l) {
           float* o = orow + fb0 + l * np;
           int n = lane / N, nd = lane - (lane / N) * N;  // off-diagonal (n, n') of p, advanced by 32 per step
@@ -340,7 +345,8 @@ __global__ void __launch_bounds__(128, 5) k_descriptor_2s(DescArgs a) {
 
 template <int L, int GN, int H>
 static int launch_descriptor(const DescArgs& a, int wpb_tuned, cudaStream_t st) {
-  const int per_warp = 4 * DescShape<L>::warp_floats(a.S, a.N);
+  const int per_warp =
+      4 * ((H == 2) ? DescShape<L>::warp_floats(a.S, a.N) : DescShape<L>::warp_floats16(a.S, a.N));
   int wpb = (200 * 1024) / per_warp;
   wpb = wpb > 4 ? 4 : wpb;
   if ((wpb_tuned == 1 || wpb_tuned == 2 || wpb_tuned == 4) && wpb_tuned <= wpb) wpb = wpb_tuned;
