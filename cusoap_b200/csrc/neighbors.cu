@@ -726,26 +726,29 @@ constexpr int kFillStage = 512;  // pairs per centre collected in shared memory
 // stable counting sort on the key (species, radial segment) and written to the
 // centre's CSR slice.  A centre with more than kFillStage pairs enumerates
 // twice instead (histogram, then scatter).  Either way the order is: by key,
-// and by candidate order within a key.
+// and by candidate order within a key.  The key is recomputed from the FP32
+// pair record whenever it is needed (the radius and segment the descriptor
+// kernels compute), so no key array takes shared memory.
 __global__ void __launch_bounds__(128) k_fill(VisitArgs A, int64_t n_centres, const int64_t* pair_off, float4* pairs,
                                               int64_t capacity, int nseg, float inv_h, int nkeys, int* status) {
   extern __shared__ __align__(16) unsigned char s_raw[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   float4* stage = reinterpret_cast<float4*>(s_raw) + (size_t)wid * kFillStage;
-  int* skey = reinterpret_cast<int*>(reinterpret_cast<float4*>(s_raw) + (size_t)(blockDim.x >> 5) * kFillStage) +
-              (size_t)wid * kFillStage;
   int* hist = reinterpret_cast<int*>(reinterpret_cast<float4*>(s_raw) + (size_t)(blockDim.x >> 5) * kFillStage) +
-              (size_t)(blockDim.x >> 5) * kFillStage + (size_t)wid * nkeys;
+              (size_t)wid * nkeys;
   int* runs = reinterpret_cast<int*>(reinterpret_cast<float4*>(s_raw) + (size_t)(blockDim.x >> 5) * kFillStage) +
-              (size_t)(blockDim.x >> 5) * (kFillStage + nkeys) + (size_t)wid * 3 * kRunsPerPass;
+              (size_t)(blockDim.x >> 5) * nkeys + (size_t)wid * 3 * kRunsPerPass;
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
   if (pair_off[n_centres] > capacity) {
     if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(status, 4);
     return;
   }
-  auto keyof = [&](int sp, double r2) {
-    const int seg = min((int)(sqrtf((float)r2) * inv_h), nseg - 1);
-    return sp * nseg + seg;
+  auto record = [](int atom, int sp, double rx, double ry, double rz) {
+    return make_float4((float)rx, (float)ry, (float)rz, __int_as_float(atom | (sp << kAtomBits)));
+  };
+  auto keyof = [&](const float4& p) {  // species * nseg + segment of the FP32 record
+    const float r = sqrtf(p.x * p.x + p.y * p.y + p.z * p.z);
+    return (int)((unsigned)__float_as_int(p.w) >> kAtomBits) * nseg + min((int)(r * inv_h), nseg - 1);
   };
   auto scan_hist = [&]() {  // exclusive scan of hist (each lane a contiguous chunk)
     const int per = (nkeys + 31) / 32;
@@ -773,15 +776,14 @@ __global__ void __launch_bounds__(128) k_fill(VisitArgs A, int64_t n_centres, co
     __syncwarp();
     if (P <= kFillStage) {
       int n = 0;
-      visit_any(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double r2) {
+      visit_any(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double) {
         const unsigned bal = __ballot_sync(0xffffffffu, ok);
         if (ok) {
           const int pos = n + __popc(bal & ((1u << lane) - 1u));
           if (pos < kFillStage) {
-            const int key = keyof(sp, r2);
-            stage[pos] = make_float4((float)rx, (float)ry, (float)rz, __int_as_float(atom | (sp << kAtomBits)));
-            skey[pos] = key;
-            atomicAdd(&hist[key], 1);
+            const float4 rec = record(atom, sp, rx, ry, rz);
+            stage[pos] = rec;
+            atomicAdd(&hist[keyof(rec)], 1);
           }
         }
         n += __popc(bal);
@@ -792,32 +794,33 @@ __global__ void __launch_bounds__(128) k_fill(VisitArgs A, int64_t n_centres, co
       for (int i0 = 0; i0 < m; i0 += 32) {
         const int i = i0 + lane;
         const bool ok = i < m;
-        const int key = ok ? skey[i] : -1 - lane;
+        const float4 rec = ok ? stage[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const int key = ok ? keyof(rec) : -1 - lane;
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         const int rank = __popc(peers & ((1u << lane) - 1u));
         const int start = ok ? hist[key] : 0;
         __syncwarp();
         if (ok) {
-          pairs[base + start + rank] = stage[i];
+          pairs[base + start + rank] = rec;
           if (rank == 0) hist[key] = start + __popc(peers);
         }
         __syncwarp();
       }
     } else {
-      visit_any(A, c, runs, [&](bool ok, int, int sp, double, double, double, double r2) {
-        if (ok) atomicAdd(&hist[keyof(sp, r2)], 1);
+      visit_any(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double) {
+        if (ok) atomicAdd(&hist[keyof(record(atom, sp, rx, ry, rz))], 1);
       });
       __syncwarp();
       scan_hist();
-      visit_any(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double r2) {
-        const int key = ok ? keyof(sp, r2) : -1 - lane;
+      visit_any(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double) {
+        const float4 rec = record(atom, sp, rx, ry, rz);
+        const int key = ok ? keyof(rec) : -1 - lane;
         const unsigned peers = __match_any_sync(0xffffffffu, key);
         const int rank = __popc(peers & ((1u << lane) - 1u));
         const int start = ok ? hist[key] : 0;
         __syncwarp();
         if (ok) {
-          pairs[base + start + rank] =
-              make_float4((float)rx, (float)ry, (float)rz, __int_as_float(atom | (sp << kAtomBits)));
+          pairs[base + start + rank] = rec;
           if (rank == 0) hist[key] = start + __popc(peers);
         }
         __syncwarp();
@@ -1019,7 +1022,7 @@ extern "C" int soapb_neighbors_fill(const soapb_basis* b, const soapb_structs* s
   NLWork w = nl_work(L, d_work);
   const VisitArgs A = visit_args(b, w, mode);
   if (c->n_centres > 0) {
-    const int smem = 4 * (16 * kFillStage + 4 * kFillStage + 4 * b->n_keys + 4 * 3 * kRunsPerPass);
+    const int smem = 4 * (16 * kFillStage + 4 * b->n_keys + 4 * 3 * kRunsPerPass);
     int rc2 = check_cuda(cudaFuncSetAttribute(k_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                          "fill smem attribute");
     if (rc2) return rc2;
