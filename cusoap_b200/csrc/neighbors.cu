@@ -568,9 +568,12 @@ __device__ __forceinline__ void visit_fine(const VisitArgs& A, int64_t c, int* r
   const double cm = A.cutoff + 1e-8;
   const double Lv[3] = {g.H[0], g.H[4], g.H[8]};
   const double cv[3] = {cp.x, cp.y, cp.z};
+  // bin coordinate u = x / (L binw) - fmin / binw (reciprocals: the 1e-8 A margin covers the rounding)
+  const double ib[3] = {1.0 / (Lv[0] * g.binw[0]), 1.0 / (Lv[1] * g.binw[1]), 1.0 / (Lv[2] * g.binw[2])};
+  const double ub[3] = {g.fmin[0] / g.binw[0], g.fmin[1] / g.binw[1], g.fmin[2] / g.binw[2]};
   // unwrapped bins of axis k that meet [x0, x1] (clamped to the grid on open axes)
   auto brange = [&](int k, double x0, double x1, int& lo, int& hi) {
-    double u0 = (x0 / Lv[k] - g.fmin[k]) / g.binw[k], u1 = (x1 / Lv[k] - g.fmin[k]) / g.binw[k];
+    double u0 = fma(x0, ib[k], -ub[k]), u1 = fma(x1, ib[k], -ub[k]);
     if (!g.per[k]) {
       u0 = fmin(fmax(u0, -1.0), (double)g.nb[k]);
       u1 = fmin(fmax(u1, -1.0), (double)g.nb[k]);
@@ -673,22 +676,30 @@ __device__ __forceinline__ void visit_fine(const VisitArgs& A, int64_t c, int* r
       int atom = 0, sp = 0;
       double rx = 0.0, ry = 0.0, rz = 0.0, r2 = 0.0;
       if (k < total) {
-        int T[3];
-        unpack3(r_T[run], T);
         const double4 p = A.sorted_pos[(int64_t)r_s0[run] + (k - r_start[run])];
         int wrap;
         unpack_info(p.w, atom, sp, wrap);
-        rx = p.x + (T[0] * Lv[0] - cp.x);
-        ry = p.y + (T[1] * Lv[1] - cp.y);
-        rz = p.z + (T[2] * Lv[2] - cp.z);
-        r2 = rx * rx + ry * ry + rz * rz;
-        ok = r2 <= A.cutoff2;
-        if (ok && g.any_per) {
-          int aw[3];
-          unpack3(wrap, aw);
+        if (!g.any_per) {  // open structure: no image shifts (warp-uniform)
+          rx = p.x - cp.x;
+          ry = p.y - cp.y;
+          rz = p.z - cp.z;
+          r2 = rx * rx + ry * ry + rz * rz;
+          ok = r2 <= A.cutoff2;
+        } else {
+          int T[3];
+          unpack3(r_T[run], T);
+          rx = p.x + (T[0] * Lv[0] - cp.x);
+          ry = p.y + (T[1] * Lv[1] - cp.y);
+          rz = p.z + (T[2] * Lv[2] - cp.z);
+          r2 = rx * rx + ry * ry + rz * rz;
+          ok = r2 <= A.cutoff2;
+          if (ok) {
+            int aw[3];
+            unpack3(wrap, aw);
 #pragma unroll
-          for (int kk = 0; kk < 3; ++kk)
-            if (g.per[kk]) ok &= abs(T[kk] - aw[kk] + cw[kk]) <= g.nrep[kk];
+            for (int kk = 0; kk < 3; ++kk)
+              if (g.per[kk]) ok &= abs(T[kk] - aw[kk] + cw[kk]) <= g.nrep[kk];
+          }
         }
         if (ok && A.mode == SOAPB_NL_CREATE && r2 <= 1e-24 && atom != ci.w) ok = false;
       }
