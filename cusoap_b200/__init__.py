@@ -4,6 +4,7 @@
 ``libsoapb200.so`` (sm_100a), reached through its C ABI (include/soapb200.h).
 """
 from .soap import SOAP
+from .xyz import read_xyz
 
-__all__ = ["SOAP"]
+__all__ = ["SOAP", "read_xyz"]
 __version__ = "0.1.0"

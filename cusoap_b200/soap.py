@@ -36,8 +36,7 @@ import torch
 from . import _lib
 from ._lib import Basis, Centres, Structs, check
 
-_SYMBOLS = {"H": 1, "He": 2, "Li": 3, "Be": 4, "B": 5, "C": 6, "N": 7, "O": 8, "F": 9, "Ne": 10, "Na": 11,
-            "Mg": 12, "Al": 13, "Si": 14, "P": 15, "S": 16, "Cl": 17, "Ar": 18, "K": 19, "Ca": 20}
+from .xyz import ATOMIC_NUMBERS as _SYMBOLS
 
 
 def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:

@@ -129,3 +129,22 @@ def test_periodic_geometries_vs_oracle(kind):
     (s.create(dict(sysd, positions=pt)) * torch.tensor(w, dtype=torch.float32, device="cuda")).sum().backward()
     Fo = o.forces(pos, Z, np.tile(w, (len(Z), 1)), cell, pbc)
     assert rel_l2(-pt.grad.cpu().numpy(), Fo) < DERIV_TOL
+
+
+def test_create_from_extended_xyz(tmp_path):
+    """A periodic structure written as extended XYZ and read back with
+    read_xyz gives exactly the descriptors of the in-memory structure."""
+    from cusoap_b200 import SOAP, read_xyz
+    P = dict(species=[1, 8], r_cut=4.5, n_max=4, l_max=3, sigma=0.5, periodic=True)
+    s = SOAP(**P)
+    sysd = _periodic_case("mixed_pbc", seed=4)
+    cell = sysd["cell"]
+    lat = " ".join(repr(float(v)) for v in np.asarray(cell).ravel())
+    pbc = " ".join("T" if p else "F" for p in sysd["pbc"])
+    lines = [str(len(sysd["atomic_numbers"])), f'Lattice="{lat}" pbc="{pbc}"']
+    sym = {1: "H", 8: "O"}
+    lines += [f"{sym[int(z)]} {x!r} {y!r} {w!r}" for z, (x, y, w) in zip(sysd["atomic_numbers"], sysd["positions"].tolist())]
+    path = tmp_path / "cell.xyz"
+    path.write_text("\n".join(lines) + "\n")
+    frame = read_xyz(str(path), index=0)
+    assert torch.equal(s.create(frame), s.create(sysd))

@@ -69,3 +69,35 @@ def test_soap_requires_cuda_device():
     from cusoap_b200 import SOAP
     with pytest.raises(ValueError):
         SOAP(species=[1], r_cut=3.0, n_max=2, l_max=1, device="cpu")
+
+
+def test_read_xyz_plain_and_extended(tmp_path):
+    import numpy as np
+    from cusoap_b200 import read_xyz
+    from cusoap_b200.xyz import atomic_number
+    rng = np.random.default_rng(3)
+    p1 = rng.uniform(0, 5, size=(3, 3))
+    p2 = rng.uniform(0, 9, size=(4, 3))
+    text = ["3", "a plain frame"]
+    text += [f"{s} {x:.10f} {y:.10f} {z:.10f}" for s, (x, y, z) in zip(["O", "H", "h"], p1)]
+    text += ["4", 'Lattice="9.0 0 0 0 9.5 0 0.5 0 10.0" Properties=species:S:1:pos:R:3 pbc="T T F" energy=-1.5']
+    text += [f"{s} {x:.10f} {y:.10f} {z:.10f} 0.0" for s, (x, y, z) in zip(["C", "8", "N", "Si"], p2)]
+    path = tmp_path / "two.xyz"
+    path.write_text("\n".join(text) + "\n")
+    frames = read_xyz(str(path))
+    assert len(frames) == 2
+    a, b = frames
+    assert np.allclose(a["positions"], p1) and list(a["atomic_numbers"]) == [8, 1, 1]
+    assert "cell" not in a and "pbc" not in a
+    assert np.allclose(b["positions"], p2) and list(b["atomic_numbers"]) == [6, 8, 7, 14]
+    assert np.allclose(b["cell"], [[9.0, 0, 0], [0, 9.5, 0], [0.5, 0, 10.0]]) and b["pbc"] == [True, True, False]
+    last = read_xyz(str(path), index=-1)
+    assert list(last["atomic_numbers"]) == [6, 8, 7, 14]
+    assert len(read_xyz(str(path), index=slice(0, 1))) == 1
+    assert atomic_number("og") == 118 and atomic_number("Fe") == 26
+    with pytest.raises(ValueError):
+        atomic_number("Xx")
+    bad = tmp_path / "bad.xyz"
+    bad.write_text("5\ncomment\nH 0 0 0\n")
+    with pytest.raises(ValueError):
+        read_xyz(str(bad))
