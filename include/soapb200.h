@@ -244,8 +244,13 @@ int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int64_t* d_pai
  * float atomics.  attach = 1: centres move with their atoms (d_centre_atom);
  * 0: fixed centres.  d_coeff: raw coefficients on SOAPB_NL_ALL pairs.
  * d_work: soapb_forces_workspace bytes (G = dE/dc per centre).  d_counter:
- * one int32 of scratch.  Replaces one reverse pass of the reference's
- * autograd Jacobian SG:2007-2113 without materialising dp/dr. */
+ * one int32 of scratch.  When d_dEdp and d_coeff are 16-byte aligned and
+ * their rows are multiples of 16 bytes, the G stage brings each centre's rows
+ * in by TMA bulk copies and waits for them at most about one second; a copy
+ * that never completes turns that block's G rows into NaN (so the forces
+ * come out NaN, not silently wrong) instead of hanging the GPU.  Replaces one
+ * reverse pass of the reference's autograd Jacobian SG:2007-2113 without
+ * materialising dp/dr. */
 int soapb_forces_workspace(const soapb_basis* b, int64_t n_centres, int64_t* bytes);
 int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
                  const float* d_coeff, const float* d_dEdp, int32_t out_mode, const int32_t* d_centre_atom,
