@@ -189,11 +189,12 @@ __device__ void cheb_to_mono(const double (&f)[kNCoef], float* dst) {
   for (int k = 0; k < kNCoef; ++k) dst[k] = (float)mono[k];
 }
 
-__global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
+__global__ void __launch_bounds__(512) k_basis_build(BasisDev a) {
   const int N = a.N, L = a.L, NF = N * (L + 1);
   __shared__ double s_gamma[(kMaxL + 1) * kMaxN];
   __shared__ double s_pref[(kMaxL + 1) * kMaxN];
   __shared__ int s_boff[kMaxS * kMaxS * (kMaxL + 1)];
+  __shared__ double s_err[4 * (kMaxL + 1) * kMaxN];
   const int tid = threadIdx.x;
 
   if (a.rbf == SOAPB_RBF_GTO) {
@@ -308,10 +309,19 @@ __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
 
   // Table error: max |table - exact| / max |exact| per function, 17 points per
   // segment over [0, cutoff]; err[0] covers B (both tables), err[1] D (the D
-  // table and the force table's derivative).
+  // table and the force table's derivative).  One task per (function,
+  // segment), maxima gathered per function in shared memory.
   for (int fn = tid; fn < NF; fn += blockDim.x) {
+    s_err[4 * fn + 0] = 0.0;  // |B error|, |D error|, max |B|, max |D|
+    s_err[4 * fn + 1] = 0.0;
+    s_err[4 * fn + 2] = 0.0;
+    s_err[4 * fn + 3] = 0.0;
+  }
+  __syncthreads();
+  for (int task = tid; task < 3 * a.nseg * NF; task += blockDim.x) {
+    const int fn = task % NF, seg = task / NF;  // seg < nseg: B and D tables; above: the force table
     double eb = 0.0, eh = 0.0, mb = 0.0, mh = 0.0;
-    for (int seg = 0; seg < a.nseg; ++seg) {
+    if (seg < a.nseg) {
       const float* cb = a.tab_b + ((size_t)seg * NF + fn) * kNCoef;
       const float* ch = a.tab_bh + ((size_t)seg * NF + fn) * kNCoef;
       for (int j = 0; j <= 16; ++j) {
@@ -327,13 +337,12 @@ __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
         mb = fmax(mb, fabs(b));
         mh = fmax(mh, fabs(bh));
       }
-    }
-    // the force table: value, and derivative d/dr = (4 / h) d/dt
-    for (int seg = 0; seg < 2 * a.nseg; ++seg) {
-      const float* cf = a.tabf + ((size_t)fn * 2 * a.nseg + seg) * kNCoef;
+    } else {  // the force table: value, and derivative d/dr = (4 / h) d/dt
+      const int sf = seg - a.nseg;
+      const float* cf = a.tabf + ((size_t)fn * 2 * a.nseg + sf) * kNCoef;
       for (int j = 0; j <= 16; ++j) {
         const double t = -1.0 + j / 8.0;
-        const double r = (seg + 0.5 * (t + 1.0)) * (0.5 * a.h);
+        const double r = (sf + 0.5 * (t + 1.0)) * (0.5 * a.h);
         if (r > a.cutoff) continue;
         double b, bh;
         exact_BD(a, s_gamma, s_pref, fn, r, b, bh);
@@ -346,6 +355,14 @@ __global__ void __launch_bounds__(256) k_basis_build(BasisDev a) {
         eh = fmax(eh, fabs(dp * 4.0 / a.h - bh));
       }
     }
+    atomic_max_nonneg(&s_err[4 * fn + 0], eb);
+    atomic_max_nonneg(&s_err[4 * fn + 1], eh);
+    atomic_max_nonneg(&s_err[4 * fn + 2], mb);
+    atomic_max_nonneg(&s_err[4 * fn + 3], mh);
+  }
+  __syncthreads();
+  for (int fn = tid; fn < NF; fn += blockDim.x) {
+    const double eb = s_err[4 * fn], eh = s_err[4 * fn + 1], mb = s_err[4 * fn + 2], mh = s_err[4 * fn + 3];
     atomic_max_nonneg(&a.err[0], mb > 0 ? eb / mb : 0.0);
     atomic_max_nonneg(&a.err[1], mh > 0 ? eh / mh : 0.0);
   }
@@ -489,7 +506,7 @@ extern "C" int soapb_basis_build(soapb_basis* b, void* dev_buf, void* stream) {
                         "polynomial grid upload");
     if (rc) return rc;
   }
-  k_basis_build<<<1, 256, 0, st>>>(a);
+  k_basis_build<<<1, 512, 0, st>>>(a);
   return check_launch("k_basis_build");
 }
 
