@@ -226,8 +226,13 @@ def test_species_errors():
                                                                               "atomic_numbers": [1]})
 
 
-def test_deterministic():
-    s = _soap("cluster192")
+@pytest.mark.parametrize("over", [{}, dict(r_cut=6.0, n_max=8, l_max=4, sigma=1.0),
+                                  dict(r_cut=6.0, n_max=8, l_max=6, sigma=0.4)])
+def test_deterministic(over):
+    """Bitwise repeatable descriptors: the two-pair-stream kernel (n_max 4,
+    l_max 3 and n_max 8, l_max 4 flush their two partial sums in a fixed
+    order) and the one-stream kernel (l_max 6)."""
+    s = _soap("cluster192", **over)
     sysd = W.make("cluster192")
     a = s.create(sysd)
     b = s.create(sysd)
