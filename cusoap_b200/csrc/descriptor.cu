@@ -16,10 +16,12 @@
 // flushes the accumulators into the warp's coefficient buffer, the segment
 // switch (warp-uniform) reloads the lane's table coefficients, so the
 // per-pair work is 7 FMAs of Horner per function plus one FMA per (n, l, m).
-// Solid harmonics are computed 16 pairs at a time (32 with two pair streams),
-// one pair per lane, into shared memory.  The power-spectrum epilogue walks the DScribe blocks
-// (species pair, l) with the m loop unrolled per l; each lane writes
-// consecutive features, so the row is stored coalesced.
+// For l_max <= 4, where one stream leaves lanes idle, each half-warp walks its
+// own stream of the pairs (k_descriptor_2s).  Solid harmonics are computed 16
+// pairs at a time (32 with two pair streams), one pair per lane, into shared
+// memory.  The power-spectrum epilogue walks the DScribe blocks (species pair,
+// l) in one non-unrolled l loop; each lane writes consecutive features, so
+// the row is stored coalesced.
 #include "common.cuh"
 
 namespace soapb {

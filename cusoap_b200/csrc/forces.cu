@@ -17,7 +17,8 @@
 //  k_adjoint_g_pipe  one block per centre iteration: the centre's dE/dp and
 //               coefficient rows arrive in shared memory by double-buffered
 //               TMA bulk copies, dE/dp is scattered into dense W_l and G[a, lm]
-//               is computed by thread-tasks (a, l).  G goes to the workspace.
+//               is computed by thread-tasks (two rows a, quad of 4 m slots).
+//               G goes to the workspace.
 //               (k_adjoint_g, with a per-basis pair -> feature index table and
 //               no dense W, serves bases whose W does not fit.)
 //  k_forces     one warp per centre (atomic work queue), ONE edge per lane:
@@ -29,7 +30,8 @@
 //               and contracts l by l:
 //                 xi_lm = sum_n G[s, n, lm] B_nl, zeta_lm = sum_n G[s, n, lm] Bhat_nl,
 //                 dE/drvec = sum_lm (rvec zeta_lm R_lm + xi_lm grad R_lm),
-//               with G broadcast from shared memory.  Neighbour forces are
+//               the last sum accumulated as five per-edge scalars, with G
+//               broadcast from shared memory.  Neighbour forces are
 //               per-lane float atomics; the centre-atom force is accumulated
 //               in registers and reduced once per centre.
 #include "common.cuh"

@@ -5,9 +5,11 @@
 // (:382-396) and _perpendicular_lengths (:369-379).  The reference
 // replicates every atom over all (2 n_rep + 1)^3 image offsets and runs an
 // all-pairs GEMM distance test; here atoms are binned once per structure
-// (counting sort into cells of perpendicular width >= the cutoff, in the
-// cell's fractional frame, periodic axes wrapped) and each centre scans only
-// the cells of its window, generating images on the fly.  The image set is
+// (counting sort into bins in the cell's fractional frame, periodic axes
+// wrapped) and each centre scans only the bins of its window, generating
+// images on the fly.  Diagonal frames use bins a quarter of the cutoff wide
+// and a window trimmed to the cutoff sphere (visit_fine); other frames use
+// bins of perpendicular width >= half the cutoff and a +-2 window (visit).  The image set is
 // the reference's: image offset n = T - w_atom + w_centre (T the cell-window
 // shift, w the wrap shifts) must satisfy |n_i| <= n_rep_i on periodic axes.
 //
