@@ -773,8 +773,9 @@ class SOAP:
                            _ptr(pairs.pair_off), _ptr(pairs.pairs), pairs.total, _ptr(coeff), _ptr(inc_row), n_inc,
                            _ptr(batch.centre_attach), int(bool(attach)), pairs.max_pairs, mode,
                            _ptr(deriv), _ptr(work), work.numel(), _ptr(status), _stream(self.device))
-                if int(status.item()) != 0:
-                    raise _lib.SoapbError(_lib.ERR_CAPACITY, "jacobian staging capacity exceeded")
+                # The kernel's per-centre entry capacity comes from pairs.max_pairs, the exact
+                # largest pair count of this list, so its overflow flag cannot be set here and is
+                # not read back: the call returns without waiting for the Jacobian to finish.
             if self.dtype != torch.float32:
                 deriv, desc = deriv.to(self.dtype), desc.to(self.dtype)
             return (deriv, desc) if return_descriptor else deriv

@@ -230,7 +230,8 @@ int soapb_jacobian_workspace(const soapb_basis* b, int64_t n_centres, int64_t n_
  * SG:2297-2301); 1: centres move with their atom (d_centre_atom), adding the
  * centre-motion term.  max_pairs: upper bound on the pairs of any centre.
  * out_mode PS or CC.  d_status: int32 flag, nonzero if a centre exceeded the
- * kernel's staging capacity.  Every edge of an atom accumulates, so periodic
+ * kernel's staging capacity (it cannot be set when max_pairs is a true upper
+ * bound, e.g. the largest count from soapb_neighbors_stats).  Every edge of an atom accumulates, so periodic
  * images are handled.  Replaces derivatives_analytical_ps SG:2270-2626 and
  * its Triton kernels SG:50-220. */
 int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
