@@ -148,3 +148,42 @@ def test_create_from_extended_xyz(tmp_path):
     path.write_text("\n".join(lines) + "\n")
     frame = read_xyz(str(path), index=0)
     assert torch.equal(s.create(frame), s.create(sysd))
+
+
+def test_jacobian_capacity_flag_at_the_c_abi():
+    """soapb_jacobian's overflow flag: with max_pairs below a centre's true
+    pair count the kernel stages what fits, sets the flag and returns; with
+    the exact count (what SOAP.derivatives passes) the flag stays 0 and the
+    result matches derivatives()."""
+    import ctypes
+    from cusoap_b200 import SOAP, _lib
+    from cusoap_b200.soap import _Batch, _Pairs, _ptr, _stream
+    s = SOAP(**W.CONFIGS["cluster192"])
+    sysd = W.water_cluster(3, 3, 3, seed=3)  # 81 atoms; the most crowded centres have 81 pairs
+    lib = _lib.load()
+    with torch.cuda.device(s.device):
+        batch = _Batch(s, [sysd], [None])
+        pairs = _Pairs(s, batch, _lib.NL_ALL)
+        _, coeff = s._run_descriptor(batch, pairs, _lib.OUT_PS, want_coeff=True)
+        n, F = batch.n_atoms, s.get_number_of_features()
+        inc_row = torch.arange(n, dtype=torch.int32, device=s.device)
+        ws = ctypes.c_int64(0)
+        _lib.check(lib.soapb_jacobian_workspace(ctypes.byref(s._basis), batch.n_centres, pairs.total, n, 0,
+                                                ctypes.byref(ws)))
+        work = torch.empty(max(int(ws.value), 256), dtype=torch.uint8, device=s.device)
+
+        def run(max_pairs):
+            out = torch.empty((batch.n_centres, n, 3, F), dtype=torch.float32, device=s.device)
+            status = torch.zeros(1, dtype=torch.int32, device=s.device)
+            _lib.check(lib.soapb_jacobian(ctypes.byref(s._basis), batch.n_centres, _ptr(pairs.pair_off),
+                                          _ptr(pairs.pairs), pairs.total, _ptr(coeff), _ptr(inc_row), n,
+                                          _ptr(batch.centre_attach), 0, max_pairs, _lib.OUT_PS, _ptr(out),
+                                          _ptr(work), work.numel(), _ptr(status), _stream(s.device)))
+            return out, int(status.item())
+
+        exact, flag = run(pairs.max_pairs)
+        assert flag == 0
+        assert torch.equal(exact, s.derivatives(sysd, return_descriptor=False))
+        assert pairs.max_pairs > 64  # the kernel's smallest staging capacity is 64 entries
+        _, flag = run(32)
+        assert flag == 1
