@@ -312,6 +312,29 @@ def test_forces_many_species_vs_oracle():
     assert rel_l2(-pt.grad.cpu().numpy(), Fo) < DERIV_TOL
 
 
+@pytest.mark.parametrize("l_max", [3, 4])
+def test_forces_without_crossover_vs_oracle(l_max):
+    """crossover=False: the adjoint's W_l has no cross-species entries (they
+    stay zero in the G kernel's shared memory); forces of E = sum w . p
+    against the oracle, with three species.  l_max 3 (F = 120) takes the TMA
+    bulk row loads, l_max 4 (F = 150) the plain ones."""
+    from cusoap_b200 import SOAP
+    rng = np.random.default_rng(13)
+    n = 45
+    pos = rng.uniform(0.0, 8.0, size=(n, 3))
+    Z = rng.choice([1, 6, 8], size=n)
+    P = dict(species=[1, 6, 8], r_cut=4.5, n_max=4, l_max=l_max, sigma=0.5, crossover=False)
+    s = SOAP(**P)
+    o = OracleSOAP(**P)
+    w = rng.standard_normal(s.get_number_of_features())
+    pt = torch.tensor(pos, device="cuda", requires_grad=True)
+    E = (s.create({"positions": pt, "atomic_numbers": Z}) * torch.tensor(w, dtype=torch.float32,
+                                                                         device="cuda")).sum()
+    E.backward()
+    Fo = o.forces(pos, Z, np.tile(w, (n, 1)))
+    assert rel_l2(-pt.grad.cpu().numpy(), Fo) < DERIV_TOL
+
+
 @pytest.mark.parametrize("n_max,l_max", [(3, 2), (5, 4)])
 def test_forces_unaligned_rows_vs_oracle(n_max, l_max):
     """Feature counts F = 63 and 275 and coefficient rows of 54 and 250 floats
