@@ -687,8 +687,16 @@ def main():
                     help="profiling case: run only the 1,000,002-atom create() leg and print its object")
     ap.add_argument("--scale-mol", type=int, default=0,
                     help="with --scale-only: cut the cluster to this many molecules (smaller profiling case)")
+    ap.add_argument("--diff-only", action="store_true",
+                    help="profiling case: run only the 2001-atom differentiation leg (forces through the "
+                         "adjoint) and print its object")
     args = ap.parse_args()
-    if args.scale_only:
+    if args.diff_only:
+        import torch
+        from cusoap_b200 import SOAP
+        torch.cuda.set_device(0)
+        print(json.dumps(diff_forces(SOAP, torch, steps=args.steps, warmup=args.warmup)), flush=True)
+    elif args.scale_only:
         import torch
         from cusoap_b200 import SOAP
         torch.cuda.set_device(0)
