@@ -440,9 +440,28 @@ def diff_forces(soap_cls, torch, steps: int = 20, warmup: int = 3):
     soap.profile = None
     ms = e0.elapsed_time(e1) / steps
     n = len(box["atomic_numbers"])
+    # the same step through the SOAP.batch graph plan (forward and adjoint replayed as graphs)
+    plan = soap.batch([box])
+
+    def graph_step():
+        pos = pos0.clone().requires_grad_(True)
+        (plan.create(pos) @ w).sum().backward()
+        return pos.grad
+
+    for _ in range(warmup):
+        graph_step()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        graph_step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms_g = e0.elapsed_time(e1) / steps
     return {"workload": "periodic water box, 2001 atoms, r_cut 6, n_max 8, l_max 6, sigma 1; E = sum w.p, forces "
                         "by create() + E.backward() (the adjoint)",
-            "atoms_per_s": n / (ms / 1e3), "ms_per_step": ms, "stage_ms_per_step": st}
+            "atoms_per_s": n / (ms / 1e3), "ms_per_step": ms, "stage_ms_per_step": st,
+            "graph_atoms_per_s": n / (ms_g / 1e3), "graph_ms_per_step": ms_g,
+            "graph_note": "the same step through SOAP.batch([box]): forward and adjoint replayed as captured graphs"}
 
 
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA at the 1965 MHz max clock
