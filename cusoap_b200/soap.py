@@ -59,6 +59,21 @@ def _resolve_z(s) -> int:
     return int(s)
 
 
+def _as_positions(x):
+    """A torch tensor stays as it is (autograd flows through it); anything
+    else becomes a float64 (n, 3) numpy array."""
+    if isinstance(x, torch.Tensor):
+        return x
+    return np.asarray(x, dtype=np.float64).reshape(-1, 3)
+
+
+def _as_numbers(x) -> np.ndarray:
+    """Atomic numbers as a host int64 array."""
+    if isinstance(x, torch.Tensor):
+        return x.detach().cpu().numpy().astype(np.int64)
+    return np.asarray(x, dtype=np.int64).reshape(-1)
+
+
 class _Weighting:
     """DScribe weighting parameters (SG:403-470); the functions themselves
     are evaluated on the device when the radial tables are built."""
@@ -130,13 +145,19 @@ class _Batch:
         cells = np.zeros((len(raw), 9))
         pbcs = np.zeros((len(raw), 3), np.uint8)
         if soap.periodic:
-            for i, r in enumerate(raw):
-                if r[2] is None or r[3] is None:
-                    raise ValueError("periodic=True requires cell and pbc.")
-                cells[i] = np.asarray(r[2].detach().cpu() if isinstance(r[2], torch.Tensor) else r[2],
-                                      dtype=np.float64).reshape(9)
-                pbcs[i] = np.asarray(r[3].detach().cpu() if isinstance(r[3], torch.Tensor) else r[3],
-                                     dtype=bool).reshape(3)
+            if any(r[2] is None or r[3] is None for r in raw):
+                raise ValueError("periodic=True requires cell and pbc.")
+            try:  # one conversion for the whole list (numpy / nested-list cells and flags)
+                if any(isinstance(r[2], torch.Tensor) or isinstance(r[3], torch.Tensor) for r in raw):
+                    raise TypeError
+                cells[:] = np.asarray([r[2] for r in raw], dtype=np.float64).reshape(len(raw), 9)
+                pbcs[:] = np.asarray([r[3] for r in raw], dtype=bool).reshape(len(raw), 3)
+            except (TypeError, ValueError):
+                for i, r in enumerate(raw):
+                    cells[i] = np.asarray(r[2].detach().cpu() if isinstance(r[2], torch.Tensor) else r[2],
+                                          dtype=np.float64).reshape(9)
+                    pbcs[i] = np.asarray(r[3].detach().cpu() if isinstance(r[3], torch.Tensor) else r[3],
+                                         dtype=bool).reshape(3)
         all_atoms = all(c is None for c in centers_list)
         # the small host arrays (and host positions) go to the device in ONE
         # asynchronous copy from a pinned staging buffer
@@ -152,6 +173,9 @@ class _Batch:
         if host_pos:
             self.positions = dev_arrays["positions"]
             self.pos_tensors = []
+        elif all(isinstance(r[0], torch.Tensor) and r[0].device == dev for r in raw):
+            # device tensors: one concatenation, one conversion
+            self.positions = torch.cat([r[0].detach() for r in raw]).to(torch.float64).contiguous()
         else:
             parts = [r[0].detach().to(dev, torch.float64) if isinstance(r[0], torch.Tensor)
                      else torch.as_tensor(r[0], dtype=torch.float64, device=dev) for r in raw]
@@ -540,28 +564,22 @@ class SOAP:
         """(positions, Z, cell, pbc) of one system (SG:291-332).  Positions
         stay a torch tensor when given as one (autograd flows through it),
         else become a float64 numpy array; Z is a host int64 array."""
-        def as_pos(x):
-            if isinstance(x, torch.Tensor):
-                return x
-            return np.asarray(x, dtype=np.float64).reshape(-1, 3)
-
-        def as_z(x):
-            if isinstance(x, torch.Tensor):
-                return x.detach().cpu().numpy().astype(np.int64)
-            return np.asarray(x, dtype=np.int64).reshape(-1)
-
+        if type(system) is dict:
+            return (_as_positions(system["positions"]), _as_numbers(system["atomic_numbers"]), system.get("cell"),
+                    system.get("pbc"))
         if isinstance(system, (tuple, list)):
             if len(system) < 2:
                 raise ValueError("Tuple/list system must be (positions, atomic_numbers, [cell], [pbc]).")
             cell = system[2] if len(system) >= 3 else None
             pbc = system[3] if len(system) >= 4 else None
-            return as_pos(system[0]), as_z(system[1]), cell, pbc
+            return _as_positions(system[0]), _as_numbers(system[1]), cell, pbc
         if isinstance(system, dict):
-            return as_pos(system["positions"]), as_z(system["atomic_numbers"]), system.get("cell"), system.get("pbc")
+            return (_as_positions(system["positions"]), _as_numbers(system["atomic_numbers"]), system.get("cell"),
+                    system.get("pbc"))
         if hasattr(system, "get_positions") and hasattr(system, "get_atomic_numbers"):
             cell = system.get_cell().array if hasattr(system, "get_cell") else None
             pbc = system.get_pbc() if hasattr(system, "get_pbc") else None
-            return as_pos(system.get_positions()), as_z(system.get_atomic_numbers()), cell, pbc
+            return _as_positions(system.get_positions()), _as_numbers(system.get_atomic_numbers()), cell, pbc
         raise TypeError("Unsupported system type. Provide ASE.Atoms-like, dict, or (positions, Z, cell, pbc).")
 
     def _species_lookup(self, Z) -> np.ndarray:
