@@ -50,6 +50,7 @@ struct ForceArgs {
   float* G;              // (n_centres, S N K) workspace
   float* forces;
   int* counter;
+  int* status;           // bit 0: a TMA row copy of the G stage timed out (G rows NaN)
   int64_t n_centres;
   int N, S, nsegf, F, attach, crossover;
   float inv_hf;  // 1 / width of a force-table segment
@@ -266,8 +267,18 @@ __global__ void __launch_bounds__(kGThreads) k_adjoint_g_pipe(ForceArgs a) {
       for (int i = tid; i < SNK; i += nth) c_dst[i] = a.coeff[c * SNK + i];
     }
     __syncthreads();
-    if (s_fail) {  // a row copy never completed: G of this block's centres is NaN
-      if (BULK && tid == 0 && next) mbar_wait(&s_bar[buf ^ 1], ((it + 1) >> 1) & 1);
+    if (s_fail) {
+      // A row copy did not complete within the wait: flag it for the host,
+      // give this block's copies still in flight (the late one and the
+      // prefetch) one more bounded wait so that none lands after the block
+      // has exited, and make G of this block's centres NaN.
+      if (tid == 0) {
+        atomicOr(a.status, 1);
+        if (BULK) {
+          mbar_wait(&s_bar[buf], (it >> 1) & 1);
+          if (next) mbar_wait(&s_bar[buf ^ 1], ((it + 1) >> 1) & 1);
+        }
+      }
       for (int64_t cc = c; cc < a.n_centres; cc += gridDim.x)
         for (int i = tid; i < SNK; i += nth) a.G[cc * SNK + i] = __int_as_float(0x7fc00000);
       return;
@@ -572,9 +583,14 @@ struct ForceDispatch {
 
 using namespace soapb;
 
-static int64_t forces_work_bytes(const soapb_basis* b, int64_t n_centres) {
+// Workspace: G (n_centres, S N K) float, then one int32 status word.
+static int64_t forces_g_bytes(const soapb_basis* b, int64_t n_centres) {
   const int64_t K = (int64_t)(b->l_max + 1) * (b->l_max + 1);
   return align_up(4 * n_centres * b->n_species * b->n_max * K, 256);
+}
+
+static int64_t forces_work_bytes(const soapb_basis* b, int64_t n_centres) {
+  return forces_g_bytes(b, n_centres) + 256;
 }
 
 extern "C" int soapb_forces_workspace(const soapb_basis* b, int64_t n_centres, int64_t* bytes) {
@@ -611,6 +627,7 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.G = (float*)d_work;
   a.forces = d_forces;
   a.counter = d_counter;
+  a.status = (int*)((char*)d_work + forces_g_bytes(b, n_centres));
   a.n_centres = n_centres;
   a.N = b->n_max;
   a.S = b->n_species;
@@ -621,5 +638,21 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.inv_hf = (float)(2.0 / b->seg_width);
   int rc = check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st), "reset work counter");
   if (rc) return rc;
+  if ((rc = check_cuda(cudaMemsetAsync(a.status, 0, sizeof(int32_t), st), "reset forces status"))) return rc;
   return dispatch_l<ForceDispatch>(b->l_max, a, b->tune[2], (int)out_mode, st);
+}
+
+extern "C" int soapb_forces_status(const soapb_basis* b, int64_t n_centres, const void* d_work, int32_t* h_status,
+                                   void* stream) {
+  if (!b || b->bytes <= 0) return set_error(SOAPB_ERR_ARG, "basis not planned");
+  if (n_centres < 0 || !d_work || !h_status) return set_error(SOAPB_ERR_ARG, "bad n_centres, workspace or status");
+  if (n_centres == 0) {
+    *h_status = 0;
+    return SOAPB_OK;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const void* p = (const char*)d_work + forces_g_bytes(b, n_centres);
+  int rc = check_cuda(cudaMemcpyAsync(h_status, p, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "forces status");
+  if (rc) return rc;
+  return check_cuda(cudaStreamSynchronize(st), "forces status sync");
 }

@@ -1093,23 +1093,63 @@ constexpr int64_t kNoAllocScratchBytes = 8ll << 20;  // 8 MiB per device
 static __device__ __align__(256) unsigned char g_nl_scratch[kNoAllocScratchBytes];
 
 static std::mutex g_scratch_mu;
-static void* g_scratch_dev_ptr[64] = {};
+struct ScratchSlot {
+  unsigned long long ctx_id;  // id of the CUDA context the address belongs to (0 = unknown)
+  void* ptr;
+};
+static ScratchSlot g_scratch_slot[64] = {};
 
-// Device address of g_nl_scratch on the current device, looked up once per
-// device (the host-side symbol is not a device address).
+// Process-unique id of the calling thread's current CUDA context, or 0 when
+// the driver cannot report one.  A device reset destroys the context (and
+// the module with g_nl_scratch); the next context gets a new id, so a cached
+// address is used only inside the context it was looked up in.  The driver
+// functions come through the runtime's entry-point query: no link to libcuda.
+static unsigned long long current_context_id() {
+  typedef int (*GetCurrentFn)(void**);
+  typedef int (*GetIdFn)(void*, unsigned long long*);
+  static GetCurrentFn get_current = nullptr;
+  static GetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 4000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = (GetCurrentFn)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = (GetIdFn)f;
+  });
+  if (!get_current || !get_id) return 0;
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != 0 || !ctx) return 0;
+  if (get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+// Device address of g_nl_scratch in the current device's context (the
+// host-side symbol is not a device address).  Looked up once per context and
+// cached: again after a cudaDeviceReset, and on every call when the context
+// id is unavailable.
 static int scratch_address(void** out) {
   int dev = 0;
   int rc = check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
   if (rc) return rc;
   if (dev < 0 || dev >= 64) return set_error(SOAPB_ERR_ARG, "device index %d out of range", dev);
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_dev_ptr[dev]) {
+  ScratchSlot& slot = g_scratch_slot[dev];
+  const unsigned long long id = current_context_id();
+  if (!slot.ptr || id == 0 || slot.ctx_id != id) {
     void* p = nullptr;
+    // also creates the device's primary context if this thread has none yet
     rc = check_cuda(cudaGetSymbolAddress(&p, g_nl_scratch), "cudaGetSymbolAddress(g_nl_scratch)");
     if (rc) return rc;
-    g_scratch_dev_ptr[dev] = p;
+    slot.ptr = p;
+    slot.ctx_id = current_context_id();
   }
-  *out = g_scratch_dev_ptr[dev];
+  *out = slot.ptr;
   return SOAPB_OK;
 }
 

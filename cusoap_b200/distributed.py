@@ -44,24 +44,37 @@ def allreduce_sum(t: torch.Tensor, group=None) -> torch.Tensor:
 
 def sharded_create(soap, system: Any, group=None):
     """This rank's centres [lo, hi) of ``system`` (every atom a centre) and
-    their descriptor rows; no collective."""
+    their descriptor rows ((0, F) for an empty shard); no collective."""
     rank, world = _world(group)
     n = len(system["atomic_numbers"]) if isinstance(system, dict) else len(system)
     lo, hi = shard_range(n, rank, world)
-    rows = soap.create(system, centers=list(range(lo, hi))) if hi > lo else None
+    if hi > lo:
+        rows = soap.create(system, centers=list(range(lo, hi)))
+    else:
+        rows = torch.zeros((0, soap.get_number_of_features()), dtype=soap.dtype, device=soap.device)
     return lo, hi, rows
 
 
 def gather_rows(rows: torch.Tensor, n_total: int, group=None) -> torch.Tensor:
-    """All ranks' descriptor rows, in centre order, on every rank."""
+    """All ranks' descriptor rows, in centre order, on every rank.
+
+    One all-gather of equal-size shards (each rank's rows padded to the
+    largest shard, at most one row of padding), so every rank receives
+    n_total rows plus the padding; the padding rows are dropped."""
     rank, world = _world(group)
     if world == 1:
         return rows
+    spans = [shard_range(n_total, r, world) for r in range(world)]
+    lo, hi = spans[rank]
+    if rows.shape[0] != hi - lo:
+        raise ValueError(f"rank {rank} holds {rows.shape[0]} rows, its shard is [{lo}, {hi})")
+    width = max(b - a for a, b in spans)
     F = rows.shape[1]
-    out = torch.zeros((n_total, F), dtype=rows.dtype, device=rows.device)
-    lo, hi = shard_range(n_total, rank, world)
-    out[lo:hi] = rows
-    return allreduce_sum(out, group)
+    send = torch.zeros((width, F), dtype=rows.dtype, device=rows.device)
+    send[:hi - lo] = rows
+    recv = torch.empty((world * width, F), dtype=rows.dtype, device=rows.device)
+    dist.all_gather_into_tensor(recv, send, group=group)
+    return torch.cat([recv[r * width:r * width + (b - a)] for r, (a, b) in enumerate(spans)])
 
 
 def partial_forces(soap, system: dict, w: torch.Tensor, lo: int, hi: int):

@@ -39,6 +39,26 @@ from ._lib import Basis, Centres, Structs, check
 from .xyz import ATOMIC_NUMBERS as _SYMBOLS
 
 
+# Parameter limits of the compiled kernels (csrc/common.cuh kMaxN, kMaxL, kMaxS).
+MAX_N_MAX, MAX_L_MAX, MAX_SPECIES = 16, 9, 16
+
+_F64_WARNED = False
+
+
+def _warn_float64():
+    """dtype='float64' returns float64 tensors, but the descriptor and its
+    derivatives are computed in float32 (about 1e-6 relative error against
+    float64, within the 1e-5 / 1e-4 tolerances); the reference computes them
+    in float64 (SG:1775-1780).  Said once per process."""
+    global _F64_WARNED
+    if not _F64_WARNED:
+        _F64_WARNED = True
+        import warnings
+        warnings.warn("cusoap_b200: dtype='float64' returns float64 tensors computed in float32 on the GPU "
+                      "(about 1e-6 relative error against float64); only the radial basis is built in float64",
+                      stacklevel=3)
+
+
 def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
     return None if t is None else t.data_ptr()
 
@@ -204,9 +224,39 @@ class _Batch:
             self.centre_struct = torch.cat(cstruct).contiguous()
             self.centre_atom = torch.cat(catom).to(torch.int32).contiguous()
             self.centre_attach = torch.cat(cattach).to(torch.int32).contiguous()
-        self.cs = Structs(len(raw), self.n_atoms, _ptr(self.atom_off), _ptr(self.positions),
+        self._describe(len(raw))
+
+    def _describe(self, n_struct: int):
+        self.cs = Structs(n_struct, self.n_atoms, _ptr(self.atom_off), _ptr(self.positions),
                           _ptr(self.species), _ptr(self.cells), _ptr(self.pbc))
         self.cc = Centres(self.n_centres, _ptr(self.centre_xyz), _ptr(self.centre_struct), _ptr(self.centre_atom))
+
+    @classmethod
+    def from_device(cls, counts_a: List[int], positions: torch.Tensor, species: torch.Tensor, cells: torch.Tensor,
+                    pbc: torch.Tensor, centre_xyz: torch.Tensor, centre_struct: torch.Tensor,
+                    centre_atom: torch.Tensor, centre_attach: torch.Tensor, counts: List[int]) -> "_Batch":
+        """A batch from arrays already on the device (structures' atoms
+        concatenated, counts_a atoms each; centres concatenated, counts per
+        structure).  No host-side adapters and no copies."""
+        self = cls.__new__(cls)
+        dev = positions.device
+        atom_off = np.concatenate([[0], np.cumsum(counts_a)]).astype(np.int64)
+        self.atom_off_list = atom_off.tolist()
+        self.n_atoms = int(atom_off[-1])
+        self.pos_tensors = []
+        self.atom_off = torch.as_tensor(atom_off).to(dev)
+        self.positions = positions.contiguous()
+        self.species = species.to(torch.int32).contiguous()
+        self.cells = cells.to(torch.float64).reshape(-1, 9).contiguous()
+        self.pbc = pbc.to(torch.uint8).reshape(-1, 3).contiguous()
+        self.counts = list(counts)
+        self.n_centres = int(sum(self.counts))
+        self.centre_xyz = centre_xyz.to(torch.float64).contiguous()
+        self.centre_struct = centre_struct.to(torch.int32).contiguous()
+        self.centre_atom = centre_atom.to(torch.int32).contiguous()
+        self.centre_attach = centre_attach.to(torch.int32).contiguous()
+        self._describe(len(counts_a))
+        return self
 
 
 class _Pairs:
@@ -420,13 +470,10 @@ class SOAP:
             raise ValueError("species must be provided (list of atomic numbers or symbols).")
         if dtype not in ("float32", "float64"):
             raise ValueError("dtype must be 'float32' or 'float64'")
+        if dtype == "float64":
+            _warn_float64()
         self._dtype_str = dtype
         self.dtype = torch.float32 if dtype == "float32" else torch.float64
-        self.device = torch.device(device) if device is not None else torch.device("cuda")
-        if self.device.type != "cuda":
-            raise ValueError("cusoap_b200 runs on CUDA devices only (no CPU fallback)")
-        if self.device.index is None:
-            self.device = torch.device("cuda", torch.cuda.current_device())
         species_Z = [_resolve_z(s) for s in species]
         self._atomic_numbers_list = sorted(set(species_Z))
         self._atomic_number_set = set(self._atomic_numbers_list)
@@ -434,6 +481,21 @@ class SOAP:
         self.n_species = len(self._atomic_numbers_list)
         self._n_max = int(n_max)
         self._l_max = int(l_max)
+        # limits of the compiled kernels (the reference has none): refused here, before any device work
+        if not 1 <= self._n_max <= MAX_N_MAX:
+            raise ValueError(f"n_max must be in [1, {MAX_N_MAX}] (the CUDA kernels are built up to n_max "
+                             f"{MAX_N_MAX}); got {self._n_max}")
+        if not 0 <= self._l_max <= MAX_L_MAX:
+            raise ValueError(f"l_max must be in [0, {MAX_L_MAX}] (the CUDA kernels are built up to l_max "
+                             f"{MAX_L_MAX}); got {self._l_max}")
+        if self.n_species > MAX_SPECIES:
+            raise ValueError(f"at most {MAX_SPECIES} species are supported (the CUDA kernels are built up to "
+                             f"{MAX_SPECIES}); got {self.n_species}")
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        if self.device.type != "cuda":
+            raise ValueError("cusoap_b200 runs on CUDA devices only (no CPU fallback)")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         self._sigma = float(sigma)
         self._eta = 1.0 / (2.0 * self._sigma * self._sigma)
         self._rbf = str(rbf).lower()
@@ -685,7 +747,21 @@ class SOAP:
                    _ptr(pairs.pairs), _ptr(coeff), _ptr(dEdp), self._out_mode() if mode is None else mode,
                    _ptr(batch.centre_attach), int(bool(attach)), _ptr(forces), _ptr(work), work.numel(),
                    _ptr(self._counter), _stream(self.device))
+        self._last_forces_work = (work, batch.n_centres)
         return forces
+
+    def forces_status(self) -> int:
+        """Status word of the last adjoint pass (synchronises the stream):
+        0 = ok; bit 0 = a row copy of its G stage did not complete within the
+        kernel's bounded wait, and the forces of that pass are NaN."""
+        last = getattr(self, "_last_forces_work", None)
+        if last is None:
+            return 0
+        work, n_centres = last
+        out = ctypes.c_int32(0)
+        check(_lib.load().soapb_forces_status(ctypes.byref(self._basis), n_centres, _ptr(work), ctypes.byref(out),
+                                              _stream(self.device)))
+        return int(out.value)
 
     def _out_mode(self) -> int:
         return _lib.OUT_CC if self.average == "cc" else _lib.OUT_PS
@@ -716,12 +792,36 @@ class SOAP:
                     return []
                 out = self._evaluate_batch(systems, centers_list)
                 parts = list(torch.split(out, [int(c) for c in self._last_counts]))
+                if self.sparse:  # each system's rows in COO, then stacked if possible (SG:1716-1737)
+                    parts = [p.to_sparse_coo() for p in parts]
                 try:
                     return torch.stack(parts, dim=0)
                 except Exception:
                     return parts
             out = self._evaluate_batch([system], [centers])
             return out.to_sparse_coo() if self.sparse else out
+
+    def create_flat(self, systems: List[Any], centers=None) -> Tuple[torch.Tensor, torch.Tensor]:
+        """Descriptors of a list of systems as ONE contiguous (total centres,
+        F) tensor and the int64 row offsets (n_systems + 1) on the host: rows
+        offsets[i]:offsets[i+1] belong to system i.  The same batched launch
+        as ``create(list)``, without splitting the output into per-system
+        views, so a caller that reduces over all systems needs no
+        concatenation.  Differentiable like ``create``; dense output.  No
+        counterpart in the reference (its list path returns per-system
+        tensors, SG:1716-1733)."""
+        systems = list(systems)
+        centers_list = [None] * len(systems) if centers is None else list(centers)
+        if len(centers_list) != len(systems):
+            raise ValueError("centers list must match number of systems.")
+        with torch.cuda.device(self.device):
+            if not systems:
+                return (torch.zeros((0, self.get_number_of_features()), dtype=self.dtype, device=self.device),
+                        torch.zeros(1, dtype=torch.int64))
+            out = self._evaluate_batch(systems, centers_list)
+            offsets = torch.zeros(len(systems) + 1, dtype=torch.int64)
+            offsets[1:] = torch.cumsum(torch.tensor(self._last_counts, dtype=torch.int64), 0)
+            return out, offsets
 
     def _evaluate_batch(self, systems, centers_list) -> torch.Tensor:
         batch = _Batch(self, systems, centers_list)
@@ -758,7 +858,9 @@ class SOAP:
         (SG:2628-2699).  "auto"/"analytical" use the closed-form kernel;
         "numerical" uses central differences of create() (step 1e-4)."""
         if method == "numerical":
-            return self.derivatives_numerical(system, centers, include, exclude, return_descriptor, attach)
+            return self.derivatives_numerical(system, centers, include, exclude, method="numerical",
+                                              return_descriptor=return_descriptor, attach=attach, n_jobs=n_jobs,
+                                              only_physical_cores=only_physical_cores, verbose=verbose)
         if method not in ("auto", "analytical"):
             raise ValueError("method must be one of: 'auto', 'analytical', 'numerical'.")
         with torch.cuda.device(self.device):
@@ -798,37 +900,100 @@ class SOAP:
                 deriv, desc = deriv.to(self.dtype), desc.to(self.dtype)
             return (deriv, desc) if return_descriptor else deriv
 
-    def derivatives_numerical(self, system, centers=None, include=None, exclude=None,
-                              return_descriptor: bool = True, attach: bool = False, d: float = 1e-4):
-        """Central differences of create() with step d (SG:1871-2003).  The
-        displaced descriptors are float32, so this is accurate to ~1e-7/d."""
+    # Default central-difference step (A) of derivatives_numerical.  The
+    # reference takes d = 1e-4 with float64 forward passes (SG:1871-1931);
+    # these forward passes are float32, whose rounding (about 1e-7 of a
+    # descriptor) divided by 2d would leave about 1e-3 relative error at
+    # d = 1e-4.  At 2e-3 A the rounding term falls to a few 1e-5 while the
+    # truncation term, (d / sigma)^2 / 6 relative for the narrowest Gaussian,
+    # stays below it for sigma >= 0.4 A.
+    FD_STEP = 2e-3
+
+    def derivatives_numerical(self, system, centers=None, include=None, exclude=None, method: str = "auto",
+                              return_descriptor: bool = True, attach: bool = False, n_jobs: int = 1,
+                              only_physical_cores: bool = False, verbose: bool = False,
+                              d: Optional[float] = None):
+        """Central differences of the descriptor (SG:1871-2003): every
+        included atom displaced by +-d along x, y, z, with DScribe's fixed
+        centres (attach=False) or index centres moving with their atom
+        (attach=True).  Returns (n_centres, n_included, 3, F), and the
+        descriptor when return_descriptor.
+
+        All 6 n_included displaced structures go through the batched path,
+        one launch per stage for as many structures as fit a fixed memory
+        budget.  The displaced descriptors are float32, so the default step
+        is ``FD_STEP`` (2e-3 A), not the reference's float64 1e-4: see the
+        note at ``FD_STEP``.  Against float64 central differences the result
+        is within about 1e-4 relative (per centre block) at the default
+        step; d = 1e-4 gives about 1e-3."""
+        if method not in ("auto", "numerical"):
+            raise ValueError("method must be 'auto' or 'numerical'.")
+        d = float(self.FD_STEP if d is None else d)
+        if not d > 0.0:
+            raise ValueError("d must be positive")
         with torch.cuda.device(self.device):
+            desc0 = self.create(system, centers) if return_descriptor else None
             pos, Z, cell, pbc = self._system_arrays(system)
             pos = (pos.detach() if isinstance(pos, torch.Tensor) else torch.as_tensor(pos)).to(self.device,
                                                                                             torch.float64)
-            n_atoms = int(pos.shape[0])
-            idx = list(range(n_atoms)) if include is None else [int(i) for i in include]
+            A = int(pos.shape[0])
+            idx = list(range(A)) if include is None else [int(i) for i in include]
             if exclude is not None:
                 ex = set(int(i) for i in exclude)
                 idx = [i for i in idx if i not in ex]
             xyz, atom, att = self._prepare_centres(pos, centers)
-            base = [xyz[k].detach().clone() for k in range(xyz.shape[0])]
-            attached = att.tolist() if attach else [-1] * len(base)
-            desc0 = self.create(system, centers) if return_descriptor else None
-            F = self.get_number_of_features()
-            deriv = torch.zeros((len(base), len(idx), 3, F), dtype=torch.float32, device=self.device)
-            for ai, a in enumerate(idx):
-                for comp in range(3):
-                    outs = []
-                    for sgn in (1.0, -1.0):
-                        p = pos.clone()
-                        p[a, comp] += sgn * d
-                        cen = [p[k] if k == a else b for k, b in zip(attached, base)]
-                        sysd = {"positions": p, "atomic_numbers": Z}
-                        if self.periodic:
-                            sysd["cell"], sysd["pbc"] = cell, pbc
-                        outs.append(self._evaluate_batch([sysd], [[c.tolist() for c in cen]]).float())
-                    deriv[:, ai, comp, :] = (outs[0] - outs[1]) / (2.0 * d)
+            C, F = int(xyz.shape[0]), self.get_number_of_features()
+            deriv = torch.zeros((C, len(idx), 3, F), dtype=torch.float32, device=self.device)
+            if not idx or C == 0:
+                deriv = deriv.to(self.dtype)
+                return (deriv, desc0) if return_descriptor else deriv
+            xyz = xyz.detach().to(torch.float64)
+            atom = atom.to(torch.int64)
+            attached = att.to(torch.int64) if attach else torch.full_like(atom, -1)
+            species = torch.as_tensor(self._species_lookup(Z)).to(self.device)
+            if self.periodic:
+                if cell is None or pbc is None:
+                    raise ValueError("periodic=True requires cell and pbc.")
+                cell_t = torch.as_tensor(np.asarray(cell.detach().cpu() if isinstance(cell, torch.Tensor) else cell,
+                                                    dtype=np.float64).reshape(9), device=self.device)
+                pbc_t = torch.as_tensor(np.asarray(pbc.detach().cpu() if isinstance(pbc, torch.Tensor) else pbc,
+                                                   dtype=bool).reshape(3).astype(np.uint8), device=self.device)
+            else:
+                cell_t = torch.zeros(9, dtype=torch.float64, device=self.device)
+                pbc_t = torch.zeros(3, dtype=torch.uint8, device=self.device)
+            # displaced structures: (atom, component) pairs in output order, each as +d then -d
+            moves = torch.tensor([(a, k) for a in idx for k in range(3)], dtype=torch.int64, device=self.device)
+            # pair-list size of one structure bounds how many structures one launch takes
+            base = _Batch.from_device([A], pos, species, cell_t, pbc_t, xyz,
+                                      torch.zeros(C, dtype=torch.int32, device=self.device), atom, attached, [C])
+            per_struct = max(_Pairs(self, base, _lib.NL_CREATE).total, 1)
+            per_move = max(1, min((1 << 26) // (2 * per_struct), (1 << 27) // (2 * C * F), (1 << 22) // (2 * A)))
+            for m0 in range(0, moves.shape[0], per_move):
+                mv = moves[m0:m0 + per_move]
+                n = 2 * mv.shape[0]
+                a_s = mv[:, 0].repeat_interleave(2)
+                k_s = mv[:, 1].repeat_interleave(2)
+                sgn = torch.tensor([d, -d], dtype=torch.float64, device=self.device).repeat(mv.shape[0])
+                P = pos.unsqueeze(0).repeat(n, 1, 1)
+                rows = torch.arange(n, device=self.device)
+                P[rows, a_s, k_s] += sgn
+                X = xyz.unsqueeze(0).repeat(n, 1, 1)
+                moved = attached.unsqueeze(0) == a_s.unsqueeze(1)  # (n, C): centres riding on the moved atom
+                X = torch.where(moved.unsqueeze(-1), P[rows, a_s].unsqueeze(1).expand(n, C, 3), X)
+                # a fixed centre stops coinciding with its atom once that atom moves (SG:966-1003)
+                lost = (atom.unsqueeze(0) == a_s.unsqueeze(1)) & ~moved
+                catom = torch.where(lost, torch.full_like(lost, -1, dtype=torch.int64), atom.unsqueeze(0))
+                catom = catom + (rows * A).unsqueeze(1) * (catom >= 0)
+                cattach = attached.unsqueeze(0) + (rows * A).unsqueeze(1) * (attached.unsqueeze(0) >= 0)
+                batch = _Batch.from_device(
+                    [A] * n, P.reshape(-1, 3), species.repeat(n), cell_t.repeat(n, 1), pbc_t.repeat(n, 1),
+                    X.reshape(-1, 3), torch.arange(n, dtype=torch.int32, device=self.device).repeat_interleave(C),
+                    catom.reshape(-1), cattach.reshape(-1), [C] * n)
+                out, _ = self._run_descriptor(batch, _Pairs(self, batch, _lib.NL_CREATE), self._out_mode())
+                out = out.view(mv.shape[0], 2, C, F).double()
+                diff = ((out[:, 0] - out[:, 1]) / (2.0 * d)).float()  # (moves, C, F)
+                # moves run over (included atom, component) in output order
+                deriv.view(C, -1, F)[:, m0:m0 + mv.shape[0], :] = diff.permute(1, 0, 2)
             deriv = deriv.to(self.dtype)
             return (deriv, desc0) if return_descriptor else deriv
 

@@ -198,8 +198,10 @@ int soapb_neighbors_clamp(int64_t* d_pair_off, int64_t n_centres, int64_t capaci
  * anything is launched.  Pairs are written only when the total
  * d_pair_off[n_centres] fits `capacity`; *d_status (device int32) receives
  * the error flags of soapb_neighbors_status (bit 2 = capacity too small).
- * The first call on each device looks up the array's device address with
- * cudaGetSymbolAddress; make that first call before any stream capture.
+ * The first call in each device's CUDA context looks up the array's device
+ * address with cudaGetSymbolAddress and caches it for that context; after a
+ * cudaDeviceReset the next call looks it up again.  Make the first call on
+ * a device (and the first after a reset) before any stream capture.
  * All calls share the one array and each call clears what must start at
  * zero; calls whose executions overlap on the GPU (other streams, other
  * threads) race on it. */
@@ -247,16 +249,23 @@ int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int64_t* d_pai
  * d_work: soapb_forces_workspace bytes (G = dE/dc per centre).  d_counter:
  * one int32 of scratch.  When d_dEdp and d_coeff are 16-byte aligned and
  * their rows are multiples of 16 bytes, the G stage brings each centre's rows
- * in by TMA bulk copies and waits for them at most about one second; a copy
- * that never completes turns that block's G rows into NaN (so the forces
- * come out NaN, not silently wrong) instead of hanging the GPU.  Replaces one
- * reverse pass of the reference's autograd Jacobian SG:2007-2113 without
- * materialising dp/dr. */
+ * in by TMA bulk copies and waits for them at most about one second.  A copy
+ * that does not complete in that time sets bit 0 of the workspace's status
+ * word (soapb_forces_status), gets one more bounded wait, and turns that
+ * block's G rows into NaN (so the forces come out NaN, not silently wrong)
+ * instead of hanging the GPU; results computed on that context afterwards
+ * should not be trusted.  Replaces one reverse pass of the reference's
+ * autograd Jacobian SG:2007-2113 without materialising dp/dr. */
 int soapb_forces_workspace(const soapb_basis* b, int64_t n_centres, int64_t* bytes);
 int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
                  const float* d_coeff, const float* d_dEdp, int32_t out_mode, const int32_t* d_centre_atom,
                  int32_t attach, float* d_forces, void* d_work, int64_t work_bytes, int32_t* d_counter,
                  void* stream);
+/* Status word of the last soapb_forces on this workspace (synchronises the
+ * stream): 0 = ok, bit 0 = a row copy of the G stage timed out.  No
+ * counterpart in the reference (autograd reports no device status). */
+int soapb_forces_status(const soapb_basis* b, int64_t n_centres, const void* d_work, int32_t* h_status,
+                        void* stream);
 
 /* Message describing the last error on the calling thread ("" if none). */
 const char* soapb_last_error(void);

@@ -64,6 +64,41 @@ def _rank_main(rank, world, port, q):
         dist.destroy_process_group()
 
 
+def _gather_main(rank, world, port, n_total, q):
+    import torch.distributed as dist
+    from cusoap_b200.distributed import gather_rows
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        lo, hi = shard_range(n_total, rank, world)
+        # stand-in descriptor rows: row i holds (i, i + 0.5, ...), so order and coverage are checkable
+        rows = torch.arange(lo, hi, dtype=torch.float32)[:, None] + 0.5 * torch.arange(5, dtype=torch.float32)
+        out = gather_rows(rows, n_total)
+        q.put((rank, out.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("n_total", [7, 8, 1])
+def test_gloo_two_ranks_gather_rows(n_total):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gather_main, args=(r, 2, port, n_total, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    want = np.arange(n_total, dtype=np.float32)[:, None] + 0.5 * np.arange(5, dtype=np.float32)
+    for r in range(2):
+        assert got[r].shape == want.shape
+        assert np.array_equal(got[r], want)
+
+
 def test_gloo_two_ranks_force_allreduce():
     ctx = mp.get_context("spawn")
     q = ctx.Queue()

@@ -1,0 +1,144 @@
+"""GPU checks of the drop-in API beyond the descriptor kernels: numerical
+derivatives against the reference's own float64 central differences,
+get_location against the reference's slices, sparse output of a list of
+systems, the flat batched output, the float64 notice and the adjoint's
+status word.  Tolerances (relative L2 per centre block): 1e-4 for
+derivatives."""
+import warnings
+
+import numpy as np
+import pytest
+import torch
+
+from cusoap_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+DERIV_TOL = 1e-4
+
+
+def _soap(name, **over):
+    from cusoap_b200 import SOAP
+    P = dict(W.CONFIGS[name])
+    P.update(over)
+    return SOAP(**P)
+
+
+def _block_err(a, b):
+    a = np.asarray(a, np.float64).reshape(a.shape[0], -1)
+    b = np.asarray(b, np.float64).reshape(b.shape[0], -1)
+    nb = np.linalg.norm(b, axis=1)
+    return float(np.max(np.linalg.norm(a - b, axis=1) / np.where(nb > 0, nb, 1.0)))
+
+
+def test_numerical_derivatives_vs_reference_fd(golden):
+    """The reference's float64 central differences (d = 1e-4) of centre 7
+    w.r.t. atoms 0..11 of the 192-atom cluster, against this float32 path at
+    its default step, and against the closed-form Jacobian."""
+    g = golden("cluster192")
+    s = _soap("cluster192")
+    sysd = {"positions": g["positions"], "atomic_numbers": g["Z"]}
+    Jn, D = s.derivatives(sysd, centers=[7], include=list(range(12)), method="numerical")
+    assert Jn.shape == g["deriv_fd"].shape
+    assert _block_err(Jn.cpu().numpy(), g["deriv_fd"]) < DERIV_TOL
+    Ja = s.derivatives(sysd, centers=[7], include=list(range(12)), return_descriptor=False)
+    assert _block_err(Jn.cpu().numpy(), Ja.cpu().numpy()) < DERIV_TOL
+    assert torch.equal(D, s.create(sysd, centers=[7]))
+
+
+def test_numerical_derivatives_attach_periodic_and_cartesian():
+    """attach=True moves index centres with their atom; a Cartesian centre
+    stays fixed; a periodic cell differentiates through its images.  Checked
+    against the closed-form Jacobian with the same conventions."""
+    s = _soap("cells512")
+    cell = W.random_cells(1, seed=11, a_min=40, a_max=40)[0]
+    inc = [0, 3, 5]
+    for attach in (False, True):
+        Jn = s.derivatives(cell, centers=[0, 5], include=inc, method="numerical", attach=attach,
+                           return_descriptor=False)
+        Ja = s.derivatives(cell, centers=[0, 5], include=inc, attach=attach, return_descriptor=False)
+        assert _block_err(Jn.cpu().numpy(), Ja.cpu().numpy()) < DERIV_TOL, attach
+    pt = [list(map(float, np.asarray(cell["positions"][2]) + 0.3))]
+    Jn = s.derivatives(cell, centers=pt, include=inc, method="numerical", return_descriptor=False)
+    Ja = s.derivatives(cell, centers=pt, include=inc, return_descriptor=False)
+    assert _block_err(Jn.cpu().numpy(), Ja.cpu().numpy()) < DERIV_TOL
+
+
+def test_numerical_derivatives_arguments():
+    s = _soap("cluster192")
+    sysd = W.make("cluster192")
+    with pytest.raises(ValueError):
+        s.derivatives_numerical(sysd, centers=[0], method="analytical")
+    with pytest.raises(ValueError):
+        s.derivatives_numerical(sysd, centers=[0], d=0.0)
+    J = s.derivatives(sysd, centers=[0, 1], include=[], method="numerical", return_descriptor=False)
+    assert J.shape == (2, 0, 3, s.get_number_of_features())
+    J = s.derivatives(sysd, centers=[0], include=[0, 1, 2], exclude=[1], method="numerical",
+                      return_descriptor=False)
+    Ja = s.derivatives(sysd, centers=[0], include=[0, 2], return_descriptor=False)
+    assert _block_err(J.cpu().numpy(), Ja.cpu().numpy()) < DERIV_TOL
+
+
+def test_get_location_golden(golden):
+    g = golden("cluster192")
+    s = _soap("cluster192")
+    for (z1, z2), key in (((1, 1), "loc_1_1"), ((1, 8), "loc_1_8"), ((8, 1), "loc_1_8"), ((8, 8), "loc_8_8")):
+        loc = s.get_location((z1, z2))
+        assert (loc.start, loc.stop) == tuple(int(v) for v in g[key]), (z1, z2)
+    assert s.get_location(("H", "O")) == s.get_location((1, 8))
+    # the slices tile the feature axis
+    spans = sorted((s.get_location(p).start, s.get_location(p).stop) for p in ((1, 1), (1, 8), (8, 8)))
+    assert spans[0][0] == 0 and spans[-1][1] == s.get_number_of_features()
+    assert all(spans[i][1] == spans[i + 1][0] for i in range(len(spans) - 1))
+    with pytest.raises(ValueError):
+        s.get_location((1, 6))
+    with pytest.raises(ValueError):
+        _soap("cluster192", average="cc").get_location((1, 8))
+
+
+def test_sparse_list_and_flat_output():
+    cells = W.random_cells(3, seed=4, a_min=10, a_max=30)
+    dense = _soap("cells512")
+    sp = _soap("cells512", sparse=True)
+    want = dense.create(cells)
+    got = sp.create(cells)
+    parts = list(got) if isinstance(got, list) else [got[i] for i in range(got.shape[0])]
+    assert len(parts) == 3
+    for p, w in zip(parts, want):
+        assert p.is_sparse
+        assert torch.equal(p.to_dense(), w)
+    same = [cells[0], cells[0]]
+    st = sp.create(same)
+    assert st.is_sparse and st.shape[0] == 2
+    flat, off = dense.create_flat(cells)
+    assert flat.is_contiguous() and off.tolist()[0] == 0 and off.tolist()[-1] == flat.shape[0]
+    for i, w in enumerate(want):
+        assert torch.equal(flat[off[i]:off[i + 1]], w)
+    # differentiable like create
+    pos = [torch.tensor(c["positions"], device="cuda", requires_grad=True) for c in cells]
+    flat, _ = dense.create_flat([dict(c, positions=p) for c, p in zip(cells, pos)])
+    flat.sum().backward()
+    assert all(p.grad is not None and torch.isfinite(p.grad).all() for p in pos)
+
+
+def test_float64_notice_and_values(monkeypatch):
+    from cusoap_b200 import soap as soap_mod
+    monkeypatch.setattr(soap_mod, "_F64_WARNED", False)
+    with pytest.warns(UserWarning, match="float32"):
+        s64 = _soap("cluster192", dtype="float64")
+    with warnings.catch_warnings():
+        warnings.simplefilter("error")
+        _soap("cluster192", dtype="float64")  # once per process
+    sysd = W.make("cluster192")
+    d64 = s64.create(sysd, centers=[0, 1])
+    assert d64.dtype == torch.float64
+    assert torch.equal(d64, _soap("cluster192").create(sysd, centers=[0, 1]).double())
+
+
+def test_forces_status_word_is_clear_after_an_adjoint():
+    s = _soap("waterbox2001")
+    box = W.water_box(8, 6.21, seed=5, dmin=2.4)
+    pos = torch.tensor(box["positions"], device="cuda", requires_grad=True)
+    s.create(dict(box, positions=pos)).sum().backward()
+    assert s.forces_status() == 0
+    assert torch.isfinite(pos.grad).all()

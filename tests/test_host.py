@@ -71,6 +71,30 @@ def test_soap_requires_cuda_device():
         SOAP(species=[1], r_cut=3.0, n_max=2, l_max=1, device="cpu")
 
 
+def test_soap_refuses_sizes_beyond_the_kernels_before_device_work():
+    """The kernels are built up to n_max 16, l_max 9 and 16 species; larger
+    requests raise ValueError naming the limit, before any CUDA call (this
+    runs without a GPU, and device=None would need one)."""
+    from cusoap_b200 import SOAP
+    from cusoap_b200.soap import MAX_L_MAX, MAX_N_MAX, MAX_SPECIES
+    with pytest.raises(ValueError, match="l_max must be in"):
+        SOAP(species=[1, 8], r_cut=5.0, n_max=4, l_max=MAX_L_MAX + 1)
+    with pytest.raises(ValueError, match="n_max must be in"):
+        SOAP(species=[1, 8], r_cut=5.0, n_max=MAX_N_MAX + 1, l_max=3)
+    with pytest.raises(ValueError, match="species"):
+        SOAP(species=list(range(1, MAX_SPECIES + 2)), r_cut=5.0, n_max=4, l_max=3)
+    # the Python limits are the library's
+    lib = _lib.load()
+    b = _lib.Basis()
+    b.n_max, b.l_max, b.n_species, b.crossover, b.r_cut, b.sigma = MAX_N_MAX, MAX_L_MAX, MAX_SPECIES, 1, 5.0, 0.5
+    assert lib.soapb_basis_plan(ctypes.byref(b)) == _lib.OK
+    for field, value in (("n_max", MAX_N_MAX + 1), ("l_max", MAX_L_MAX + 1), ("n_species", MAX_SPECIES + 1)):
+        c = _lib.Basis()
+        c.n_max, c.l_max, c.n_species, c.crossover, c.r_cut, c.sigma = 4, 3, 2, 1, 5.0, 0.5
+        setattr(c, field, value)
+        assert lib.soapb_basis_plan(ctypes.byref(c)) == _lib.ERR_ARG, field
+
+
 def test_read_xyz_plain_and_extended(tmp_path):
     import numpy as np
     from cusoap_b200 import read_xyz
