@@ -15,11 +15,13 @@ HBM, CUDA events around every step, max over ranks); ``e2e`` is the same
 call with the positions copied from pinned host memory and both outputs
 copied back to pinned host memory inside the timed region; ``roofline`` is
 the Jacobian kernel (an HBM write stream) timed with CUDA events during the
-timed steps; ``cpu_baseline`` is the FP64 oracle restatement of the
-reference's CPU path on a bounded sample.  Under torchrun each rank runs its
-own copy of the workload (weak scaling, no data-path collective).
-``--impl reference`` times the reference's CPU algorithm (the oracle port;
-the reference itself is Python and does not travel) on the host cores.
+timed steps; ``cpu_baseline`` is the reference's algorithm (its timed CPU
+port, oracle/reference_port.py) on a bounded sample of its own centre-batch
+loop, on every host thread.  Under torchrun each rank runs its own copy of
+the workload (weak scaling, no data-path collective).  ``--impl reference``
+times that port step by step, every step in full: create + analytical
+derivatives of 50 consecutive centres (the reference itself is Python and
+does not travel to the benchmark host).
 """
 from __future__ import annotations
 
@@ -42,11 +44,15 @@ UNIT = "atoms/s"
 WORKLOAD = "cluster3000"
 CONFIG = {
     "workload": "(H2O)_1000 non-periodic water cluster, 3000 atoms; species H,O; r_cut=10, n_max=7, l_max=3, "
-                "sigma=0.5, gto, average=off; create + analytical dP/dr (3000 x 3000 x 3 x 420 float32)",
-    "atoms_per_step": 3000,
+                "sigma=0.5, gto, average=off; create + analytical dP/dr of every centre w.r.t. every atom "
+                "(float32 output)",
     "features": 420,
-    "l2": "each step writes 45.4 GB (> 126 MB L2); L2 also flushed between timed steps",
+    "l2": "GPU arm: each step writes 45.4 GB (> 126 MB L2) and L2 is also flushed between timed steps",
 }
+# Centres per step of the reference arm: the reference's own driver loops over
+# centre batches, create(centers=range(s, e)) + derivatives(same centres)
+# (examples/test_serial.py:53-60).
+REF_BATCH = 50
 
 
 def _peaks():
@@ -187,33 +193,58 @@ def _dist():
 
 
 def parity_centres(n_centres: int = 24):
-    """The sampled centres of the CPU baseline (and of the Jacobian parity check)."""
+    """The sampled centres of the Jacobian parity check."""
     rng = np.random.default_rng(0)
     return [int(c) for c in rng.choice(3000, n_centres, replace=False)]
 
 
-def cpu_baseline_sample(n_centres: int = 24, workers: int = 1):
-    """Oracle (FP64 numpy restatement of the reference path) on a bounded
-    sample: create over all 3000 centres plus the dense Jacobian of
-    n_centres centres; scaled to atoms/s of the full step.  Also returns the
-    oracle's outputs, the checker of the GPU step's parity."""
-    from oracle.soap_oracle import OracleSOAP
-    from cusoap_b200 import workloads as W
-    sysd = W.make(WORKLOAD)
-    o = OracleSOAP(**W.CONFIGS[WORKLOAD])
+def _host_threads() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+def _reference_steps(port, sysd, n_steps: int, first: int = 0):
+    """n_steps steps of the reference's centre-batch loop on the port:
+    create + analytical derivatives of REF_BATCH consecutive centres per
+    step.  Step i takes batch (23 i) mod n_batches (a permutation of the
+    batches, as 23 is prime to 60), so a few steps sample the whole cluster,
+    surface and interior, not only its first lattice rows.  Returns
+    per-step seconds and centres."""
     pos, Z = sysd["positions"], sysd["atomic_numbers"]
-    t0 = time.perf_counter()
-    desc = o.create(pos, Z)
-    t_create = time.perf_counter() - t0
-    cen = parity_centres(n_centres)
-    t0 = time.perf_counter()
-    jac = o.derivatives(pos, Z, centers=cen, return_descriptor=False)
-    t_der = time.perf_counter() - t0
-    per_atom = t_create / 3000 + t_der / n_centres
-    return {"value": 1.0 / per_atom, "unit": UNIT, "cores": workers, "kind": "port",
-            "sample": f"oracle create of all 3000 centres ({t_create:.2f} s) + dense FP64 Jacobian of "
-                      f"{n_centres} sampled centres ({t_der:.2f} s), scaled to one full step",
-            "seconds": t_create + t_der}, desc, jac
+    n = len(Z)
+    n_batches = (n + REF_BATCH - 1) // REF_BATCH
+    times, counts = [], []
+    for i in range(first, first + n_steps):
+        s = ((23 * i) % n_batches) * REF_BATCH
+        cen = list(range(s, min(s + REF_BATCH, n)))
+        t0 = time.perf_counter()
+        port.create(pos, Z, cen)
+        port.derivatives(pos, Z, cen)
+        times.append(time.perf_counter() - t0)
+        counts.append(len(cen))
+    return times, counts
+
+
+def cpu_baseline_sample(n_steps: int = 2):
+    """The reference's algorithm (its timed CPU port, float64 inside,
+    float32 out, on every host thread) on a bounded sample: n_steps steps of
+    its centre-batch loop.  Also returns the float64 checker values of the
+    GPU step's parity: every descriptor row, and the Jacobian blocks of the
+    parity centres."""
+    import torch
+    from oracle.reference_port import ReferencePort
+    from cusoap_b200 import workloads as W
+    threads = _host_threads()
+    torch.set_num_threads(threads)
+    sysd = W.make(WORKLOAD)
+    port = ReferencePort(**W.CONFIGS[WORKLOAD])
+    times, counts = _reference_steps(port, sysd, n_steps)
+    check = ReferencePort(**W.CONFIGS[WORKLOAD], out_dtype=torch.float64)
+    desc = check.create(sysd["positions"], sysd["atomic_numbers"]).numpy()
+    jac = check.derivatives(sysd["positions"], sysd["atomic_numbers"], parity_centres()).numpy()
+    return {"value": sum(counts) / sum(times), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n_steps} steps of the reference's centre-batch loop (create + analytical dP/dr of "
+                      f"{REF_BATCH} centres per step) on its timed CPU port, {sum(times):.2f} s",
+            "seconds": sum(times)}, desc, jac
 
 
 def _row_err(a, b) -> float:
@@ -258,59 +289,81 @@ def parity_other_legs(soap_cls, torch):
     return out
 
 
-def _ref_worker(args):
-    kind, centres = args
-    from oracle.soap_oracle import OracleSOAP
-    from cusoap_b200 import workloads as W
-    sysd = W.make(WORKLOAD)
-    o = OracleSOAP(**W.CONFIGS[WORKLOAD])
-    t0 = time.perf_counter()
-    if kind == "create":
-        o.create(sysd["positions"], sysd["atomic_numbers"], centers=centres)
-    else:
-        o.derivatives(sysd["positions"], sysd["atomic_numbers"], centers=centres, return_descriptor=False)
-    return time.perf_counter() - t0
-
-
 def run_reference(args):
-    """--impl reference: the reference's CPU algorithm (oracle port) on all
-    host cores, one bounded sample per step."""
-    import multiprocessing as mp
+    """--impl reference: the reference's algorithm on the host CPU, as its
+    own driver runs it (examples/test_serial.py:53-60): every step is
+    create + analytical derivatives of a batch of REF_BATCH consecutive
+    centres, executed in full and timed.  The reference is a Python package
+    that does not travel to the benchmark host, so its timed CPU port runs
+    (oracle/reference_port.py: the same torch float64 operations, timed
+    against the reference itself on the same threads by
+    oracle/calibrate_port.py).  Under torchrun only rank 0 runs."""
+    import torch
     world, rank, _ = _dist()
     if rank != 0:
         return
-    workers = os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    rng = np.random.default_rng(1)
-    per_step = []
-    with ctx.Pool(workers) as pool:
-        def one_step():
-            chunks = np.array_split(np.arange(3000), workers)
-            dcen = [int(c) for c in rng.choice(3000, 2 * workers, replace=False)]
-            t0 = time.perf_counter()
-            pool.map(_ref_worker, [("create", [int(x) for x in ch]) for ch in chunks])
-            t_create = time.perf_counter() - t0
-            t0 = time.perf_counter()
-            pool.map(_ref_worker, [("deriv", dcen[k::workers]) for k in range(workers)])
-            t_der = time.perf_counter() - t0
-            # the sampled Jacobian rows scale linearly with the centre count
-            return t_create + t_der * 3000 / len(dcen)
-        for _ in range(max(1, args.warmup)):
-            one_step()
-        for _ in range(args.steps):
-            per_step.append(one_step())
-    t = sum(per_step) / len(per_step)
-    value = 3000.0 / t
+    from oracle.reference_port import ReferencePort
+    from cusoap_b200 import workloads as W
+    threads = _host_threads()
+    torch.set_num_threads(threads)
+    sysd = W.make(WORKLOAD)
+    port = ReferencePort(**W.CONFIGS[WORKLOAD])
+    _reference_steps(port, sysd, max(0, args.warmup))
+    times, counts = _reference_steps(port, sysd, args.steps, first=max(0, args.warmup))
+    t = sum(times)
+    value = sum(counts) / t
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": dict(CONFIG, parallelism="host cores"),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
-                             "sample": f"per step: oracle create of all 3000 centres + dense FP64 Jacobian of "
-                                       f"{2 * workers} sampled centres, scaled to 3000 centres; {workers} "
-                                       f"spawned worker processes"},
+            "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "impl": "reference", "config": dict(CONFIG), "atoms_per_step": REF_BATCH,
+            "parallelism": f"{threads} host threads",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"every step in full: create + analytical dP/dr of {REF_BATCH} consecutive "
+                                       f"centres (the reference's centre-batch loop) on its timed CPU port, float64 "
+                                       f"inside, float32 out; {args.steps} steps, {t:.2f} s timed"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def plain_cpu_cluster192(soap_cls, torch):
+    """The CPU workload of the reference (192-atom (H2O)_64 cluster, n_max 4,
+    l_max 3, r_cut 5, sigma 0.5): create + analytical derivatives of every
+    centre w.r.t. every atom in float64, on the reference's timed CPU port
+    with every host thread; beside it the same call on the GPU path
+    (float32 arithmetic)."""
+    from oracle.reference_port import ReferencePort
+    from cusoap_b200 import workloads as W
+    sysd = W.make("cluster192")
+    pos, Z = sysd["positions"], sysd["atomic_numbers"]
+    threads = _host_threads()
+    torch.set_num_threads(threads)
+    port = ReferencePort(**W.CONFIGS["cluster192"], out_dtype=torch.float64)
+    ts = []
+    for _ in range(4):
+        t0 = time.perf_counter()
+        port.create(pos, Z)
+        port.derivatives(pos, Z)
+        ts.append(time.perf_counter() - t0)
+    t_cpu = statistics.median(ts[1:])
+    soap = soap_cls(**W.CONFIGS["cluster192"])
+    pos_d = torch.tensor(pos, device="cuda")
+    for _ in range(3):
+        soap.derivatives({"positions": pos_d, "atomic_numbers": Z})
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(20):
+        soap.derivatives({"positions": pos_d, "atomic_numbers": Z})
+    e1.record()
+    torch.cuda.synchronize()
+    t_gpu = e0.elapsed_time(e1) / 20 / 1e3
+    n = len(Z)
+    return {"workload": "(H2O)_64 non-periodic cluster, 192 atoms; r_cut 5, n_max 4, l_max 3, sigma 0.5; create + "
+                        "analytical derivatives of every centre w.r.t. every atom",
+            "cpu_port_atoms_per_s": n / t_cpu, "cpu_port_s": t_cpu, "cpu_threads": threads, "cpu_dtype": "f64",
+            "gpu_atoms_per_s": n / t_gpu, "gpu_ms": t_gpu * 1e3, "gpu_dtype": "f32",
+            "note": "CPU: the reference's algorithm on its timed port, median of 3 after one warm-up; GPU: "
+                    "SOAP.derivatives on device-resident positions, 20 calls after 3 warm-ups"}
 
 
 def batched_vs_plain(soap_cls, torch):
@@ -333,8 +386,8 @@ def batched_vs_plain(soap_cls, torch):
             d = dict(c)
             d["positions"] = c["positions"].clone().requires_grad_(True)
             sysl.append(d)
-        out = soap.create(sysl)  # a list: the cells differ in size
-        E = ((torch.cat(out) if isinstance(out, list) else out) @ w).sum()
+        out, _ = soap.create_flat(sysl)  # one (total atoms, F) buffer for the whole batch
+        E = (out @ w).sum()
         E.backward()
         return sysl
 
@@ -353,11 +406,10 @@ def batched_vs_plain(soap_cls, torch):
         return pos
 
     res = {}
-    for name, fn in (("batched", batched), ("graph", graph), ("plain", plain)):
+    for name, fn, reps in (("batched", batched, 20), ("graph", graph, 20), ("plain", plain, 5)):
         fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = 3
         e0.record()
         for _ in range(reps):
             fn()
@@ -658,6 +710,13 @@ def run_ours(args):
         except Exception as exc:
             diff = {"error": repr(exc)}
 
+    plain192 = None
+    if not args.no_batched and rank == 0 and world == 1 and args.nx == 10 and not args.no_cpu:
+        try:
+            plain192 = plain_cpu_cluster192(SOAP, torch)
+        except Exception as exc:  # reported, never silently dropped
+            plain192 = {"error": repr(exc)}
+
     cpu = None
     parity = None
     if want_parity:
@@ -665,8 +724,8 @@ def run_ours(args):
         parity = {"tolerance": {"descriptor": 1e-5, "derivative": 1e-4},
                   "headline_desc_max_row_rel_l2": _row_err(par_D, o_desc),
                   "headline_jacobian_max_centre_rel_l2": _row_err(par_J, o_jac),
-                  "note": "relative L2 against the FP64 oracle: every descriptor row of the last timed step, and the "
-                          "Jacobian blocks of the 24 centres the CPU baseline samples"}
+                  "note": "relative L2 against float64 (the reference's port with float64 output): every "
+                          "descriptor row of the last timed step, and the Jacobian blocks of 24 sampled centres"}
         del o_desc, o_jac
         try:
             parity.update(parity_other_legs(SOAP, torch))
@@ -681,10 +740,12 @@ def run_ours(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": dict(CONFIG, parallelism=f"replicas x{world}" if world > 1 else "single GPU")
-            if args.nx == 10 else {"workload": f"profiling case: {n_at}-atom water cluster, same parameters"},
+            "config": dict(CONFIG) if args.nx == 10
+            else {"workload": f"profiling case: {n_at}-atom water cluster, same parameters"},
+            "atoms_per_step": n_at, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk, "cpu_baseline": cpu,
-            "batched_vs_plain": extra, "scale_create": scale, "diff_forces": diff, "parity_vs_fp64": parity}
+            "batched_vs_plain": extra, "scale_create": scale, "diff_forces": diff, "plain_cpu_cluster192": plain192,
+            "parity_vs_fp64": parity}
     print(json.dumps(line), flush=True)
 
 
