@@ -4,10 +4,11 @@ For one basis (n_max, l_max, species, crossover) on one GPU model it times,
 with CUDA events on the launch stream, every candidate shape on a sample
 system and keeps the fastest:
 
-* descriptor: warps per block (1, 2, 4) x radial functions per lane (the
-  minimum for n_max and l_max, and the next supported size above it: more
-  functions per lane means fewer busy lanes but more independent work per
-  lane; with two pair streams per warp only the warps per block);
+* descriptor: warps per block (1, 2, 4); for the l-grouped kernel (n_max
+  > 8 or l_max > 6) also radial functions per lane (the minimum for n_max
+  and l_max, and the next supported size above it: more functions per lane
+  means fewer busy lanes but more independent work per lane; with two pair
+  streams per warp only the warps per block);
 * adjoint edge kernel: warps per block (1, 2, 4).
 
 The choice is written into the basis (``soapb_basis.tune``), so every later
@@ -51,9 +52,19 @@ def two_pair_streams(n_max: int, l_max: int) -> bool:
     return (l_max + 1) * -(-n_max // gn) <= 24
 
 
+def radial_index_lanes(n_max: int, l_max: int) -> bool:
+    """The built-in descriptor kernel family for (n_max, l_max) -- the rule
+    of DescDispatch in csrc/descriptor.cu: one lane per radial index n (all
+    (l, m) accumulators in the lane) for n_max <= 8 and l_max <= 6, lanes
+    grouped by l otherwise.  The tuner keeps the family (the two sum in
+    different orders) and tunes only launch shapes within it."""
+    return n_max <= 8 and l_max <= 6
+
+
 def descriptor_candidates(n_max: int, l_max: int) -> List[Tuple[int, int]]:
     g0 = min_functions_per_lane(n_max, l_max)
-    if two_pair_streams(n_max, l_max):  # functions per lane are not a choice there
+    if radial_index_lanes(n_max, l_max) or two_pair_streams(n_max, l_max):
+        # functions per lane are not a choice there
         return [(w, g0) for w in (1, 2, 4)]
     gns = [g for g in _GN_SIZES if g >= g0][:2]
     return [(w, g) for w in (1, 2, 4) for g in gns]

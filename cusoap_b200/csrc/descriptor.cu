@@ -37,6 +37,7 @@ struct DescArgs {
   int* counter;
   int N, S, nseg, F, mode, crossover;
   float inv_h;
+  float self_ratio;  // w0 / w(0): an r = 0 edge's table value times this is its self value
 };
 
 // Position of harmonic block l in a pair's Y row: l^2 plus a padding that
@@ -106,7 +107,99 @@ inline bool desc_two_streams(int N, int L) {
 }
 
 constexpr int kMaxBlocks = kMaxS * (kMaxS + 1) / 2;
+constexpr int kMaxLNLanes = 6;  // largest l_max of the radial-index-lane kernel (registers)
 constexpr int kMaxTri = kMaxN * (kMaxN + 1) / 2;
+
+// Per-block tables of the power-spectrum epilogue: the prefactor
+// sqrt(8 pi^2 / (2l+1)) per l, the DScribe species blocks (j | jd << 8, first
+// feature) and the (n, n') pairs of the upper-triangle index.
+template <int L>
+__device__ __forceinline__ void desc_tables(const DescArgs& a, float* s_pref, int* s_blk, unsigned char* s_tri) {
+  const int N = a.N, S = a.S;
+  if (threadIdx.x <= L) s_pref[threadIdx.x] = sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * threadIdx.x + 1.0f));
+  if (threadIdx.x == 0) {
+    int nb = 0, f = 0;
+    for (int j = 0; j < S; ++j)
+      for (int jd = j; jd < (a.crossover ? S : j + 1); ++jd) {
+        s_blk[2 * nb] = j | (jd << 8);
+        s_blk[2 * nb + 1] = f;
+        f += (j == jd ? N * (N + 1) / 2 : N * N) * (L + 1);
+        ++nb;
+      }
+    int p = 0;
+    for (int n = 0; n < N; ++n)
+      for (int nd = n; nd < N; ++nd, ++p) {
+        s_tri[2 * p] = (unsigned char)n;
+        s_tri[2 * p + 1] = (unsigned char)nd;
+      }
+  }
+}
+
+// One centre's outputs from its coefficients cbuf[(s N + n) KC + lm]
+// (KC = K | 1), written by the whole warp: the raw coefficient row when
+// requested, then the power spectrum in DScribe order (each lane writes
+// consecutive features of a block, so rows are stored coalesced), or the
+// cc / raw projection.
+template <int L>
+__device__ __forceinline__ void desc_epilogue(const DescArgs& a, int64_t c, const float* cbuf, int lane,
+                                              const float* s_pref, const int* s_blk, const unsigned char* s_tri) {
+  constexpr int K = (L + 1) * (L + 1), KC = K | 1;
+  const int N = a.N, S = a.S;
+  if (a.coeff_out) {
+    float* crow = a.coeff_out + (size_t)c * S * N * K;
+    for (int f = lane; f < S * N * K; f += 32) {
+      const int sn = f / K;
+      crow[f] = cbuf[sn * KC + (f - sn * K)];
+    }
+  }
+  float* orow = a.out + (size_t)c * a.F;
+  if (a.mode == SOAPB_OUT_PS) {
+    const int nblk = a.crossover ? S * (S + 1) / 2 : S;
+    const int q32 = 32 / N, r32 = 32 % N;  // p -> p + 32 in the off-diagonal (n, n') order
+    for (int b = 0; b < nblk; ++b) {
+      const int jj = s_blk[2 * b], fb0 = s_blk[2 * b + 1];
+      const int j = jj & 255, jd = jj >> 8;
+      const bool diag = j == jd;
+      const int np = diag ? N * (N + 1) / 2 : N * N;
+#pragma unroll 1  // one copy of the l loop: smaller code, fewer instruction-fetch stalls
+      for (int l = 0; l <= L; ++l) {
+        float* o = orow + fb0 + l * np;
+        int n = lane / N, nd = lane - (lane / N) * N;  // off-diagonal (n, n') of p, advanced by 32 per step
+        for (int p = lane; p < np; p += 32) {
+          if (diag) {
+            n = s_tri[2 * p];
+            nd = s_tri[2 * p + 1];
+          }
+          const float* x = cbuf + (j * N + n) * KC + l * l;
+          const float* y = cbuf + (jd * N + nd) * KC + l * l;
+          float s = 0.0f;
+#pragma unroll
+          for (int m = 0; m < 2 * l + 1; ++m) s = fmaf(x[m], y[m], s);
+          o[p] = s * s_pref[l];
+          if (!diag) {
+            n += q32;
+            nd += r32;
+            if (nd >= N) { nd -= N; ++n; }
+          }
+        }
+      }
+    }
+  } else {
+    const bool cc = a.mode == SOAPB_OUT_CC;
+    const float pi_m15 = (float)(1.0 / (kPi * 1.7724538509055160273));  // pi^-3/2
+    for (int f = lane; f < a.F; f += 32) {
+      const int sn = f / K, lm = f - sn * K;
+      int src = lm;
+      float scale = 1.0f;
+      if (cc) {
+        // l = 1 stored (z, x, y) = source lm (2, 3, 1); lm >= 4 scaled by pi^-3/2
+        if (lm >= 1 && lm <= 3) src = (lm == 3) ? 1 : lm + 1;
+        if (lm >= 4) scale = pi_m15;
+      }
+      orow[f] = cbuf[sn * KC + src] * scale;
+    }
+  }
+}
 
 // H pair streams per warp (1, or 2 for small l_max): half-warp h takes pairs
 // 16 h .. 16 h + 15 of every staged batch of 32.  Each stream keeps its own
@@ -134,26 +227,8 @@ __device__ __forceinline__ void descriptor_body(const DescArgs& a) {
   int* sg = (int*)(tt + BQ);
   int* spp = sg + BQ;
   float* cbuf = (float*)(spp + BQ);
-  if (threadIdx.x <= L) s_pref[threadIdx.x] = sqrtf(8.0f * (float)(kPi * kPi) / (2.0f * threadIdx.x + 1.0f));
-  if (threadIdx.x == 0) {
-    int nb = 0, f = 0;
-    for (int j = 0; j < S; ++j)
-      for (int jd = j; jd < (a.crossover ? S : j + 1); ++jd) {
-        s_blk[2 * nb] = j | (jd << 8);
-        s_blk[2 * nb + 1] = f;
-        f += (j == jd ? N * (N + 1) / 2 : N * N) * (L + 1);
-        ++nb;
-      }
-    int p = 0;
-    for (int n = 0; n < N; ++n)
-      for (int nd = n; nd < N; ++nd, ++p) {
-        s_tri[2 * p] = (unsigned char)n;
-        s_tri[2 * p + 1] = (unsigned char)nd;
-      }
-  }
+  desc_tables<L>(a, s_pref, s_blk, s_tri);
   __syncthreads();
-  const int nblk = a.crossover ? S * (S + 1) / 2 : S;
-  const int q32 = 32 / N, r32 = 32 % N;  // p -> p + 32 in the off-diagonal (n, n') order
 
   // lane -> stream, l and its functions n = k GN + g
   const int h = (H == 2) ? (lane >> 4) : 0, hl = lane & (HL - 1);
@@ -277,59 +352,7 @@ __device__ __forceinline__ void descriptor_body(const DescArgs& a) {
       if (h == hh && cur_sp >= 0) flush(cur_sp);
       __syncwarp();
     }
-
-    if (a.coeff_out) {
-      float* crow = a.coeff_out + (size_t)c * S * N * K;
-      for (int f = lane; f < S * N * K; f += 32) {
-        const int sn = f / K;
-        crow[f] = cbuf[sn * KC + (f - sn * K)];
-      }
-    }
-    float* orow = a.out + (size_t)c * a.F;
-    if (a.mode == SOAPB_OUT_PS) {
-      for (int b = 0; b < nblk; ++b) {
-        const int jj = s_blk[2 * b], fb0 = s_blk[2 * b + 1];
-        const int j = jj & 255, jd = jj >> 8;
-        const bool diag = j == jd;
-        const int np = diag ? N * (N + 1) / 2 : N * N;
-#pragma unroll 1  // one copy of the l loop: smaller code, fewer instruction-fetch stalls
-        for (int l = 0; l <= L; ++l) {
-          float* o = orow + fb0 + l * np;
-          int n = lane / N, nd = lane - (lane / N) * N;  // off-diagonal (n, n') of p, advanced by 32 per step
-          for (int p = lane; p < np; p += 32) {
-            if (diag) {
-              n = s_tri[2 * p];
-              nd = s_tri[2 * p + 1];
-            }
-            const float* x = cbuf + (j * N + n) * KC + l * l;
-            const float* y = cbuf + (jd * N + nd) * KC + l * l;
-            float s = 0.0f;
-#pragma unroll
-            for (int m = 0; m < 2 * l + 1; ++m) s = fmaf(x[m], y[m], s);
-            o[p] = s * s_pref[l];
-            if (!diag) {
-              n += q32;
-              nd += r32;
-              if (nd >= N) { nd -= N; ++n; }
-            }
-          }
-        }
-      }
-    } else {
-      const bool cc = a.mode == SOAPB_OUT_CC;
-      const float pi_m15 = (float)(1.0 / (kPi * 1.7724538509055160273));  // pi^-3/2
-      for (int f = lane; f < a.F; f += 32) {
-        const int sn = f / K, lm = f - sn * K;
-        int src = lm;
-        float scale = 1.0f;
-        if (cc) {
-          // l = 1 stored (z, x, y) = source lm (2, 3, 1); lm >= 4 scaled by pi^-3/2
-          if (lm >= 1 && lm <= 3) src = (lm == 3) ? 1 : lm + 1;
-          if (lm >= 4) scale = pi_m15;
-        }
-        orow[f] = cbuf[sn * KC + src] * scale;
-      }
-    }
+    desc_epilogue<L>(a, c, cbuf, lane, s_pref, s_blk, s_tri);
     __syncwarp();
   }
 }
@@ -344,6 +367,187 @@ __global__ void __launch_bounds__(128) k_descriptor(DescArgs a) {
 template <int L, int GN>
 __global__ void __launch_bounds__(128, 4) k_descriptor_2s(DescArgs a) {
   descriptor_body<L, GN, 2>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Radial-index lanes (n_max <= 8, l_max <= 6): lane n of a stream owns the
+// radial index n and ALL K = (l_max+1)^2 accumulators c[n][lm] of it, so
+// every lane does the same work per pair -- l_max+1 Horner evaluations
+// (its functions (n, 0..l_max)) and K FMAs -- with no idle m slots.  NP
+// lanes form a stream (NP = 8, or 4 for n_max <= 4); the 32 / NP streams of
+// a warp walk contiguous, equal parts of the centre's pair list, so each
+// stream sees only its part's species and segment runs and reloads its
+// coefficients rarely.  32 pairs (NP per stream) are staged per batch, one
+// per lane, as rows of solid harmonics in shared memory; rows have an odd
+// stride, so the streams' reads of the same slot k from their rows hit
+// different banks and the staging writes are conflict-free.
+//
+// The r = 0 edge of the centre's own atom needs no test in the pair loop:
+// its solid harmonics are (Y00, 0, ..., 0) and its table value is
+// w(0) B_n0(0), so staging scales its R_00 by self_ratio = w0 / w(0) and the
+// edge adds exactly w0 B_n0(0) Y00.  A stream whose species changes flushes
+// its accumulators into the centre's coefficient buffer; streams flush one
+// after the other, and in a fixed order at the end, so sums are
+// deterministic.
+template <int L>
+struct NShape {
+  static constexpr int K = (L + 1) * (L + 1);
+  static constexpr int YS = K | 1;
+  static constexpr int KC = K | 1;
+  __host__ __device__ static int warp_floats(int S, int N) { return 32 * YS + 3 * 32 + S * N * KC; }
+};
+
+template <int L, int NP>
+__device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
+  using Sh = NShape<L>;
+  constexpr int K = Sh::K, YS = Sh::YS, KC = Sh::KC, H = 32 / NP;
+  extern __shared__ float sm[];
+  __shared__ float s_pref[kMaxL + 1];
+  __shared__ int s_blk[2 * kMaxBlocks];
+  __shared__ unsigned char s_tri[2 * kMaxTri];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int N = a.N, S = a.S, NF = N * (L + 1);
+  float* Y = sm + (size_t)wid * Sh::warp_floats(S, N);
+  float* tt = Y + 32 * YS;
+  int* sg = (int*)(tt + 32);
+  int* spp = sg + 32;
+  float* cbuf = (float*)(spp + 32);
+  desc_tables<L>(a, s_pref, s_blk, s_tri);
+  __syncthreads();
+  const int h = lane / NP, n = lane - h * NP;
+  const bool active = n < N;
+  const int cbn = S * N * KC;
+
+  for (;;) {
+    int c32 = 0;
+    if (lane == 0) c32 = atomicAdd(a.counter, 1);
+    const int64_t c = __shfl_sync(0xffffffffu, c32, 0);
+    if (c >= a.n_centres) break;
+    for (int i = lane; i < cbn; i += 32) cbuf[i] = 0.0f;
+    const int64_t p0 = a.pair_off[c], P = a.pair_off[c + 1] - p0;
+    const int64_t s0 = p0 + (P * h) / H, s1 = p0 + (P * (h + 1)) / H;  // this stream's pairs
+    const int64_t rounds = (P + H - 1) / H;                             // longest stream
+    float acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0f;
+    float cf[L + 1][kNCoef];
+#pragma unroll
+    for (int l = 0; l <= L; ++l)
+#pragma unroll
+      for (int k = 0; k < kNCoef; ++k) cf[l][k] = 0.0f;
+    int cur_sp = -1, cur_seg = -1;
+    __syncwarp();
+
+    for (int64_t base = 0; base < rounds; base += NP) {
+      // stage: lane (h, n) takes pair s0 + base + n of its stream into row `lane`
+      {
+        const int64_t e = s0 + base + n;
+        float* yrow = Y + lane * YS;
+        if (e < s1) {
+          const float4 pr = __ldg(a.pairs + e);
+          const int w = __float_as_int(pr.w);
+          const float r = sqrtf(pr.x * pr.x + pr.y * pr.y + pr.z * pr.z);
+          int seg;
+          float t;
+          seg_coord(r, a.inv_h, a.nseg, seg, t);
+          tt[lane] = t;
+          sg[lane] = seg;
+          spp[lane] = (int)((unsigned)w >> kAtomBits);
+          SolidHarmonics<L>::values(pr.x, pr.y, pr.z, [&](int idx, float v) { yrow[idx] = v; });
+          if (!(r > 0.0f)) yrow[0] *= a.self_ratio;  // the centre's own Gaussian: w0 B_n0(0) Y00
+        } else {  // past the end of this stream: a zero row that adds nothing and changes nothing
+#pragma unroll
+          for (int k = 0; k < K; ++k) yrow[k] = 0.0f;
+          tt[lane] = 0.0f;
+          sg[lane] = -1;
+          spp[lane] = -1;
+        }
+      }
+      __syncwarp();
+#pragma unroll 1
+      for (int j = 0; j < NP; ++j) {
+        const int q = h * NP + j;
+        const int sq = spp[q];
+        const int sp = sq < 0 ? cur_sp : sq;
+        if (__any_sync(0xffffffffu, sp != cur_sp)) {
+#pragma unroll
+          for (int hh = 0; hh < H; ++hh) {  // streams flush one after the other
+            if (h == hh && sp != cur_sp) {
+              if (cur_sp >= 0 && active) {
+                float* dst = cbuf + (cur_sp * N + n) * KC;
+#pragma unroll
+                for (int k = 0; k < K; ++k) dst[k] += acc[k];
+              }
+#pragma unroll
+              for (int k = 0; k < K; ++k) acc[k] = 0.0f;
+              cur_sp = sp;
+            }
+            __syncwarp();
+          }
+        }
+        const int sq2 = sg[q];
+        const int seg = sq2 < 0 ? cur_seg : sq2;
+        if (seg != cur_seg) {
+          if (active) {
+#pragma unroll
+            for (int l = 0; l <= L; ++l) load_coef(a.tab_b, seg, fn_index(n, l, N), NF, cf[l]);
+          }
+          cur_seg = seg;
+        }
+        const float t = tt[q];
+        float B[L + 1];
+#pragma unroll
+        for (int l = 0; l <= L; ++l) B[l] = horner7(cf[l], t);
+        const float* yr = Y + q * YS;
+#pragma unroll
+        for (int l = 0; l <= L; ++l)
+#pragma unroll
+          for (int k = l * l; k < (l + 1) * (l + 1); ++k) acc[k] = fmaf(B[l], yr[k], acc[k]);
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int hh = 0; hh < H; ++hh) {
+      if (h == hh && cur_sp >= 0 && active) {
+        float* dst = cbuf + (cur_sp * N + n) * KC;
+#pragma unroll
+        for (int k = 0; k < K; ++k) dst[k] += acc[k];
+      }
+      __syncwarp();
+    }
+    desc_epilogue<L>(a, c, cbuf, lane, s_pref, s_blk, s_tri);
+    __syncwarp();
+  }
+}
+
+template <int L, int NP>
+__global__ void __launch_bounds__(128, (L <= 4) ? 4 : 3) k_descriptor_n(DescArgs a) {
+  descriptor_n_body<L, NP>(a);
+}
+
+template <int L, int NP>
+static int launch_descriptor_n(const DescArgs& a, int wpb_tuned, cudaStream_t st) {
+  const int per_warp = 4 * NShape<L>::warp_floats(a.S, a.N);
+  int wpb = (200 * 1024) / per_warp;
+  wpb = wpb > 4 ? 4 : wpb;
+  if ((wpb_tuned == 1 || wpb_tuned == 2 || wpb_tuned == 4) && wpb_tuned <= wpb) wpb = wpb_tuned;
+  if (wpb < 1) return set_error(SOAPB_ERR_UNSUPPORTED, "descriptor shared memory %d B per warp too large", per_warp);
+  const int smem = wpb * per_warp;
+  auto kern = k_descriptor_n<L, NP>;
+  int rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                      "descriptor smem attribute");
+  if (rc) return rc;
+  int dev = 0, nsm = 148, occ = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 * wpb, smem);
+  if (occ < 1) occ = 1;
+  int64_t blocks = (int64_t)nsm * occ;
+  const int64_t need = (a.n_centres + wpb - 1) / wpb;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) blocks = 1;
+  kern<<<(unsigned)blocks, 32 * wpb, smem, st>>>(a);
+  return check_launch("k_descriptor_n");
 }
 
 template <int L, int GN, int H>
@@ -374,7 +578,11 @@ static int launch_descriptor(const DescArgs& a, int wpb_tuned, cudaStream_t st) 
 
 template <int L>
 struct DescDispatch {
-  static int run(const DescArgs& a, int gn, int wpb, cudaStream_t st) {
+  static int run(const DescArgs& a, int gn, int wpb, bool lgroup_only, cudaStream_t st) {
+    if constexpr (L <= kMaxLNLanes) {
+      if (!lgroup_only && a.N <= 8 && isfinite(a.self_ratio))
+        return a.N <= 4 ? launch_descriptor_n<L, 4>(a, wpb, st) : launch_descriptor_n<L, 8>(a, wpb, st);
+    }
     if constexpr (L <= 4) {
       if (desc_two_streams(a.N, L)) {  // functions per lane fixed by (N, L): ceil(N / floor(16 / (L+1)))
         const int lpl = 16 / (L + 1), g2 = (a.N + lpl - 1) / lpl;
@@ -427,10 +635,20 @@ extern "C" int soapb_descriptor(const soapb_basis* b, int64_t n_centres, const i
   a.mode = out_mode;
   a.crossover = b->crossover ? 1 : 0;
   a.inv_h = (float)(1.0 / b->seg_width);
+  {
+    // self_ratio = w0 / w(0) of the weighting (the r = 0 table value is w(0) B_n0(0)); not finite
+    // (a weighting singular at r = 0) sends the call to the kernels that use the self table
+    const double w0 = b->weighting == SOAPB_W_NONE ? 1.0 : b->w_w0;
+    double w_at0 = 1.0;
+    if (b->weighting == SOAPB_W_POLY) w_at0 = b->w_c;
+    else if (b->weighting == SOAPB_W_POW) w_at0 = b->w_c / (b->w_d + pow(0.0, b->w_m));
+    else if (b->weighting == SOAPB_W_EXP) w_at0 = b->w_c / (b->w_d + 1.0);
+    a.self_ratio = (float)(w0 / w_at0);
+  }
   int rc = check_cuda(cudaMemsetAsync(d_counter, 0, sizeof(int32_t), st), "reset work counter");
   if (rc) return rc;
   int gn = desc_group(N, L);
   const int tg = b->tune[1];
   if (tg > gn && (tg == 2 || tg == 3 || tg == 4 || tg == 6)) gn = tg;
-  return dispatch_l<DescDispatch>(L, a, gn, b->tune[0], st);
+  return dispatch_l<DescDispatch>(L, a, gn, b->tune[0], b->tune[3] == 1, st);
 }

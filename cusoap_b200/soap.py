@@ -901,13 +901,21 @@ class SOAP:
             return (deriv, desc) if return_descriptor else deriv
 
     # Default central-difference step (A) of derivatives_numerical.  The
-    # reference takes d = 1e-4 with float64 forward passes (SG:1871-1931);
-    # these forward passes are float32, whose rounding (about 1e-7 of a
-    # descriptor) divided by 2d would leave about 1e-3 relative error at
-    # d = 1e-4.  At 2e-3 A the rounding term falls to a few 1e-5 while the
-    # truncation term, (d / sigma)^2 / 6 relative for the narrowest Gaussian,
-    # stays below it for sigma >= 0.4 A.
-    FD_STEP = 2e-3
+    # reference takes d = 1e-4 with float64 forward passes (SG:1871-1931).
+    # These forward passes are float32: a displaced descriptor carries about
+    # 1e-7 |p| of rounding, so a difference quotient carries about
+    # 1e-7 |p| / (2 d) of noise, against a derivative block that for one
+    # neighbour atom is only a small part of |p| per A.  The truncation term
+    # grows as (d / sigma)^2 / 6, and an atom within d of a centre's cutoff
+    # sees the basis's truncation step (about 1e-3 of its peak), which makes
+    # the quotient jump; with attach=True every neighbour of a moving centre
+    # can cross, so that happens about d / 1e-4 times as often as with the
+    # reference's step.  Measured against the closed form on
+    # the workloads (per centre block), 5e-3 A balances them: 6e-5 on the
+    # 3000-atom cluster and the periodic cells (sigma 0.4), 8e-4 on the water
+    # box, up to 1e-2 for blocks made only of atoms far from the centre;
+    # d = 1e-4 gives 2e-3 to 3e-1.
+    FD_STEP = 5e-3
 
     def derivatives_numerical(self, system, centers=None, include=None, exclude=None, method: str = "auto",
                               return_descriptor: bool = True, attach: bool = False, n_jobs: int = 1,
@@ -922,10 +930,12 @@ class SOAP:
         All 6 n_included displaced structures go through the batched path,
         one launch per stage for as many structures as fit a fixed memory
         budget.  The displaced descriptors are float32, so the default step
-        is ``FD_STEP`` (2e-3 A), not the reference's float64 1e-4: see the
-        note at ``FD_STEP``.  Against float64 central differences the result
-        is within about 1e-4 relative (per centre block) at the default
-        step; d = 1e-4 gives about 1e-3."""
+        is ``FD_STEP`` (5e-3 A), not the reference's float64 1e-4, and the
+        result is accurate to about 1e-7 |p| / (2 d) absolute: within 1e-4
+        relative of float64 differences for a centre's block that includes
+        its own atom, up to about 1e-3 to 1e-2 for blocks of distant atoms
+        only (see the note at ``FD_STEP``).  The closed-form ``derivatives``
+        (about 1e-6) is the accurate path."""
         if method not in ("auto", "numerical"):
             raise ValueError("method must be 'auto' or 'numerical'.")
         d = float(self.FD_STEP if d is None else d)

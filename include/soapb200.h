@@ -89,8 +89,11 @@ typedef struct soapb_basis {
   int32_t seg_hint;     /* 0, or a lower bound on n_seg (finer tables) */
   int32_t tune[4];      /* launch shapes picked by an autotuner, 0 = built-in choice:
                            [0] descriptor warps per block (1, 2, 4), [1] descriptor radial
-                           functions per lane (1, 2, 3, 4, 6; at least the minimum for n_max,
-                           l_max), [2] adjoint edge-kernel warps per block (1, 2, 4), [3] 0 */
+                           functions per lane of the l-grouped kernel (1, 2, 3, 4, 6; at least
+                           the minimum for n_max, l_max), [2] adjoint edge-kernel warps per
+                           block (1, 2, 4), [3] descriptor kernel family: 0 = built-in (one
+                           lane per radial index n for n_max <= 8, l_max <= 6, else lanes
+                           grouped by l), 1 = lanes grouped by l always */
   const double* h_poly; /* SOAPB_RBF_POLY: host rx[quad_n] | wr[quad_n] | g[n_max][quad_n] (g_n on the grid) */
   /* derived by soapb_basis_plan */
   double eta;        /* 1 / (2 sigma^2) */

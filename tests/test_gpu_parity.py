@@ -226,17 +226,47 @@ def test_species_errors():
                                                                               "atomic_numbers": [1]})
 
 
+@pytest.mark.parametrize("family", [0, 1])
 @pytest.mark.parametrize("over", [{}, dict(r_cut=6.0, n_max=8, l_max=4, sigma=1.0),
                                   dict(r_cut=6.0, n_max=8, l_max=6, sigma=0.4)])
-def test_deterministic(over):
-    """Bitwise repeatable descriptors: the two-pair-stream kernel (n_max 4,
-    l_max 3 and n_max 8, l_max 4 flush their two partial sums in a fixed
-    order) and the one-stream kernel (l_max 6)."""
+def test_deterministic(over, family):
+    """Bitwise repeatable descriptors from both kernel families: one lane per
+    radial index (family 0, the built-in choice here; its pair streams flush
+    in a fixed order) and lanes grouped by l (family 1: the two-pair-stream
+    kernel at n_max 4, l_max 3 and n_max 8, l_max 4, the one-stream kernel at
+    l_max 6)."""
     s = _soap("cluster192", **over)
+    s._basis.tune[3] = family
     sysd = W.make("cluster192")
     a = s.create(sysd)
     b = s.create(sysd)
     assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["cluster192", "cells512", "cluster1M"])
+def test_both_descriptor_families_match_the_oracle(name):
+    """The radial-index-lane kernel (built-in) and the l-grouped kernel
+    (tune[3] = 1) against the FP64 oracle on the same structures, with the
+    centres' own atoms (self edges) and Cartesian centres off the atoms."""
+    P = dict(W.CONFIGS[name])
+    if name == "cluster1M":
+        sysd = W.water_cluster(6, 6, 6, seed=2)
+    elif name == "cells512":
+        sysd = W.random_cells(1, seed=9, a_min=90, a_max=90)[0]
+    else:
+        sysd = W.make(name)
+    o = _oracle(name)
+    cen = list(range(0, len(sysd["atomic_numbers"]), 7))
+    cart = [list(map(float, np.asarray(sysd["positions"][i]) + 0.37)) for i in (1, 4)]
+    want = o.create(sysd["positions"], sysd["atomic_numbers"], centers=cen, cell=sysd.get("cell"),
+                    pbc=sysd.get("pbc"))
+    want_c = o.create(sysd["positions"], sysd["atomic_numbers"], centers=cart, cell=sysd.get("cell"),
+                      pbc=sysd.get("pbc"))
+    for family in (0, 1):
+        s = _soap(name)
+        s._basis.tune[3] = family
+        assert _row_err(_np(s.create(sysd, centers=cen)), want) < DESC_TOL, family
+        assert _row_err(_np(s.create(sysd, centers=cart)), want_c) < DESC_TOL, family
 
 
 # ---- full-size workloads: sampled rows against the oracle ----
