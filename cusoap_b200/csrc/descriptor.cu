@@ -389,34 +389,38 @@ __global__ void __launch_bounds__(128, 4) k_descriptor_2s(DescArgs a) {
 // its accumulators into the centre's coefficient buffer; streams flush one
 // after the other, and in a fixed order at the end, so sums are
 // deterministic.
-template <int L>
+template <int L, int NP>
 struct NShape {
   static constexpr int K = (L + 1) * (L + 1);
-  static constexpr int YS = K | 1;
+  static constexpr int K4 = (K + 3) & ~3;  // row length in floats: float4 reads and writes
+  static constexpr int H = 32 / NP;
   static constexpr int KC = K | 1;
-  __host__ __device__ static int warp_floats(int S, int N) { return 32 * YS + 3 * 32 + S * N * KC; }
+  // row q = h NP + j starts at q K4 + 4 h: the H streams' float4 reads of the
+  // same slot fall on different groups of four banks whatever K4 is
+  static constexpr int YF = 32 * K4 + 4 * H;
+  // a multiple of 4 floats, so every warp's rows stay 16-byte aligned for the float4 accesses
+  __host__ __device__ static int warp_floats(int S, int N) { return (YF + 4 * 32 + S * N * KC + 3) & ~3; }
 };
 
 template <int L, int NP>
 __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
-  using Sh = NShape<L>;
-  constexpr int K = Sh::K, YS = Sh::YS, KC = Sh::KC, H = 32 / NP;
-  extern __shared__ float sm[];
+  using Sh = NShape<L, NP>;
+  constexpr int K = Sh::K, K4 = Sh::K4, KC = Sh::KC, H = Sh::H;
+  extern __shared__ __align__(16) float sm[];
   __shared__ float s_pref[kMaxL + 1];
   __shared__ int s_blk[2 * kMaxBlocks];
   __shared__ unsigned char s_tri[2 * kMaxTri];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int N = a.N, S = a.S, NF = N * (L + 1);
   float* Y = sm + (size_t)wid * Sh::warp_floats(S, N);
-  float* tt = Y + 32 * YS;
-  int* sg = (int*)(tt + 32);
-  int* spp = sg + 32;
-  float* cbuf = (float*)(spp + 32);
+  float4* meta = reinterpret_cast<float4*>(Y + Sh::YF);  // per staged pair: t, segment, species
+  float* cbuf = Y + Sh::YF + 4 * 32;
   desc_tables<L>(a, s_pref, s_blk, s_tri);
   __syncthreads();
   const int h = lane / NP, n = lane - h * NP;
   const bool active = n < N;
   const int cbn = S * N * KC;
+  float4* myrow = reinterpret_cast<float4*>(Y + lane * K4 + 4 * h);  // the row this lane stages
 
   for (;;) {
     int c32 = 0;
@@ -442,7 +446,10 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
       // stage: lane (h, n) takes pair s0 + base + n of its stream into row `lane`
       {
         const int64_t e = s0 + base + n;
-        float* yrow = Y + lane * YS;
+        float yv[K4];
+#pragma unroll
+        for (int k = 0; k < K4; ++k) yv[k] = 0.0f;
+        float4 m = make_float4(0.0f, __int_as_float(-1), __int_as_float(-1), 0.0f);
         if (e < s1) {
           const float4 pr = __ldg(a.pairs + e);
           const int w = __float_as_int(pr.w);
@@ -450,24 +457,20 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
           int seg;
           float t;
           seg_coord(r, a.inv_h, a.nseg, seg, t);
-          tt[lane] = t;
-          sg[lane] = seg;
-          spp[lane] = (int)((unsigned)w >> kAtomBits);
-          SolidHarmonics<L>::values(pr.x, pr.y, pr.z, [&](int idx, float v) { yrow[idx] = v; });
-          if (!(r > 0.0f)) yrow[0] *= a.self_ratio;  // the centre's own Gaussian: w0 B_n0(0) Y00
-        } else {  // past the end of this stream: a zero row that adds nothing and changes nothing
+          m = make_float4(t, __int_as_float(seg), __int_as_float((int)((unsigned)w >> kAtomBits)), 0.0f);
+          SolidHarmonics<L>::values(pr.x, pr.y, pr.z, [&](int idx, float v) { yv[idx] = v; });
+          if (!(r > 0.0f)) yv[0] *= a.self_ratio;  // the centre's own Gaussian: w0 B_n0(0) Y00
+        }  // past the end of this stream: a zero row that adds nothing and changes nothing
 #pragma unroll
-          for (int k = 0; k < K; ++k) yrow[k] = 0.0f;
-          tt[lane] = 0.0f;
-          sg[lane] = -1;
-          spp[lane] = -1;
-        }
+        for (int k4 = 0; k4 < K4 / 4; ++k4) myrow[k4] = make_float4(yv[4 * k4], yv[4 * k4 + 1], yv[4 * k4 + 2], yv[4 * k4 + 3]);
+        meta[lane] = m;
       }
       __syncwarp();
 #pragma unroll 1
       for (int j = 0; j < NP; ++j) {
         const int q = h * NP + j;
-        const int sq = spp[q];
+        const float4 m = meta[q];
+        const int sq = __float_as_int(m.z);
         const int sp = sq < 0 ? cur_sp : sq;
         if (__any_sync(0xffffffffu, sp != cur_sp)) {
 #pragma unroll
@@ -485,7 +488,7 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
             __syncwarp();
           }
         }
-        const int sq2 = sg[q];
+        const int sq2 = __float_as_int(m.y);
         const int seg = sq2 < 0 ? cur_seg : sq2;
         if (seg != cur_seg) {
           if (active) {
@@ -494,15 +497,24 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
           }
           cur_seg = seg;
         }
-        const float t = tt[q];
         float B[L + 1];
 #pragma unroll
-        for (int l = 0; l <= L; ++l) B[l] = horner7(cf[l], t);
-        const float* yr = Y + q * YS;
+        for (int l = 0; l <= L; ++l) B[l] = horner7(cf[l], m.x);
+        const float4* yr = reinterpret_cast<const float4*>(Y + q * K4 + 4 * h);
 #pragma unroll
-        for (int l = 0; l <= L; ++l)
+        for (int k4 = 0; k4 < K4 / 4; ++k4) {
+          const float4 v = yr[k4];
+          const float vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-          for (int k = l * l; k < (l + 1) * (l + 1); ++k) acc[k] = fmaf(B[l], yr[k], acc[k]);
+          for (int i = 0; i < 4; ++i) {
+            const int k = 4 * k4 + i;
+            if (k < K) {
+              int l = 0;
+              while ((l + 1) * (l + 1) <= k) ++l;  // compile time: k is unrolled
+              acc[k] = fmaf(B[l], vv[i], acc[k]);
+            }
+          }
+        }
       }
       __syncwarp();
     }
@@ -527,7 +539,8 @@ __global__ void __launch_bounds__(128, (L <= 4) ? 4 : 3) k_descriptor_n(DescArgs
 
 template <int L, int NP>
 static int launch_descriptor_n(const DescArgs& a, int wpb_tuned, cudaStream_t st) {
-  const int per_warp = 4 * NShape<L>::warp_floats(a.S, a.N);
+  const int per_warp = 4 * NShape<L, NP>::warp_floats(a.S, a.N);
+  if (per_warp % 16 != 0) return set_error(SOAPB_ERR_ARG, "descriptor: warp slice of %d B not 16-byte aligned", per_warp);
   int wpb = (200 * 1024) / per_warp;
   wpb = wpb > 4 ? 4 : wpb;
   if ((wpb_tuned == 1 || wpb_tuned == 2 || wpb_tuned == 4) && wpb_tuned <= wpb) wpb = wpb_tuned;
