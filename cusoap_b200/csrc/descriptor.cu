@@ -208,7 +208,7 @@ __device__ __forceinline__ void desc_epilogue(const DescArgs& a, int64_t c, cons
 template <int L, int GN, int H>
 __device__ __forceinline__ void descriptor_body(const DescArgs& a) {
   using Sh = DescShape<L>;
-  constexpr int K = Sh::K, YS = Sh::YS, KC = Sh::KC, M = 2 * L + 1;
+  constexpr int YS = Sh::YS, KC = Sh::KC, M = 2 * L + 1;
   constexpr int HL = 32 / H;           // lanes per stream
   constexpr int LPL = HL / (L + 1);    // lanes per l
   constexpr int HOFF = (H == 2) ? Sh::HOFF : 0;
@@ -402,6 +402,33 @@ struct NShape {
   __host__ __device__ static int warp_floats(int S, int N) { return (YF + 4 * 32 + S * N * KC + 3) & ~3; }
 };
 
+// One pair's contribution to a radial-index lane: the lane's l_max + 1 radial
+// functions at t (Horner), then acc[lm] += B_l R_lm over the pair's harmonic
+// row, read as float4.
+template <int L, int K4>
+__device__ __forceinline__ void accumulate_pair(float (&acc)[(L + 1) * (L + 1)], const float (&cf)[L + 1][kNCoef],
+                                                float t, const float* yrow) {
+  constexpr int K = (L + 1) * (L + 1);
+  float B[L + 1];
+#pragma unroll
+  for (int l = 0; l <= L; ++l) B[l] = horner7(cf[l], t);
+  const float4* yr = reinterpret_cast<const float4*>(yrow);
+#pragma unroll
+  for (int k4 = 0; k4 < K4 / 4; ++k4) {
+    const float4 v = yr[k4];
+    const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int k = 4 * k4 + i;
+      if (k < K) {
+        int l = 0;
+        while ((l + 1) * (l + 1) <= k) ++l;  // compile time: k is unrolled
+        acc[k] = fmaf(B[l], vv[i], acc[k]);
+      }
+    }
+  }
+}
+
 template <int L, int NP>
 __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
   using Sh = NShape<L, NP>;
@@ -413,7 +440,9 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int N = a.N, S = a.S, NF = N * (L + 1);
   float* Y = sm + (size_t)wid * Sh::warp_floats(S, N);
-  float4* meta = reinterpret_cast<float4*>(Y + Sh::YF);  // per staged pair: t, segment, species
+  float* tt = Y + Sh::YF;  // per staged pair: segment coordinate t, segment, species
+  int* sg = reinterpret_cast<int*>(tt + 32);
+  int* spp = sg + 32;
   float* cbuf = Y + Sh::YF + 4 * 32;
   desc_tables<L>(a, s_pref, s_blk, s_tri);
   __syncthreads();
@@ -444,78 +473,95 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
 
     for (int64_t base = 0; base < rounds; base += NP) {
       // stage: lane (h, n) takes pair s0 + base + n of its stream into row `lane`
+      const int64_t e = s0 + base + n;
+      const bool valid = e < s1;
+      const int nvalid = (int)max((int64_t)0, min((int64_t)NP, s1 - (s0 + base)));  // this stream's block
+      int seg = -1, sp = -1;
+      float t = 0.0f;
       {
-        const int64_t e = s0 + base + n;
         float yv[K4];
 #pragma unroll
         for (int k = 0; k < K4; ++k) yv[k] = 0.0f;
-        float4 m = make_float4(0.0f, __int_as_float(-1), __int_as_float(-1), 0.0f);
-        if (e < s1) {
+        if (valid) {
           const float4 pr = __ldg(a.pairs + e);
-          const int w = __float_as_int(pr.w);
           const float r = sqrtf(pr.x * pr.x + pr.y * pr.y + pr.z * pr.z);
-          int seg;
-          float t;
           seg_coord(r, a.inv_h, a.nseg, seg, t);
-          m = make_float4(t, __int_as_float(seg), __int_as_float((int)((unsigned)w >> kAtomBits)), 0.0f);
+          sp = (int)((unsigned)__float_as_int(pr.w) >> kAtomBits);
           SolidHarmonics<L>::values(pr.x, pr.y, pr.z, [&](int idx, float v) { yv[idx] = v; });
           if (!(r > 0.0f)) yv[0] *= a.self_ratio;  // the centre's own Gaussian: w0 B_n0(0) Y00
-        }  // past the end of this stream: a zero row that adds nothing and changes nothing
+        }  // past the end of this stream: a zero row that adds nothing
 #pragma unroll
-        for (int k4 = 0; k4 < K4 / 4; ++k4) myrow[k4] = make_float4(yv[4 * k4], yv[4 * k4 + 1], yv[4 * k4 + 2], yv[4 * k4 + 3]);
-        meta[lane] = m;
+        for (int k4 = 0; k4 < K4 / 4; ++k4)
+          myrow[k4] = make_float4(yv[4 * k4], yv[4 * k4 + 1], yv[4 * k4 + 2], yv[4 * k4 + 3]);
       }
+      // rows past the end repeat the segment and species of the block's last pair (or the
+      // stream's current ones), so they change nothing; then one bit per row marks where
+      // the segment or the species differs from the stream's previous row
+      const int last = h * NP + (nvalid > 0 ? nvalid - 1 : 0);
+      const int seg_last = __shfl_sync(0xffffffffu, seg, last), sp_last = __shfl_sync(0xffffffffu, sp, last);
+      if (!valid) {
+        seg = nvalid > 0 ? seg_last : cur_seg;
+        sp = nvalid > 0 ? sp_last : cur_sp;
+      }
+      int seg_prev = __shfl_up_sync(0xffffffffu, seg, 1), sp_prev = __shfl_up_sync(0xffffffffu, sp, 1);
+      if (n == 0) {
+        seg_prev = cur_seg;
+        sp_prev = cur_sp;
+      }
+      const unsigned seg_chg = __ballot_sync(0xffffffffu, seg != seg_prev);
+      const unsigned sp_chg = __ballot_sync(0xffffffffu, sp != sp_prev);
+      tt[lane] = t;
+      sg[lane] = seg;
+      spp[lane] = sp;
       __syncwarp();
+      if (sp_chg == 0) {
+        // no species change in any stream: t, a coefficient reload where the segment changes,
+        // Horner and the K FMAs per pair
+#pragma unroll 2
+        for (int j = 0; j < NP; ++j) {
+          const int q = h * NP + j;
+          if ((seg_chg >> q) & 1u) {
+            const int sq = sg[q];
+            if (active) {
+#pragma unroll
+              for (int l = 0; l <= L; ++l) load_coef(a.tab_b, sq, fn_index(n, l, N), NF, cf[l]);
+            }
+          }
+          accumulate_pair<L, K4>(acc, cf, tt[q], Y + q * K4 + 4 * h);
+        }
+      } else {
 #pragma unroll 1
-      for (int j = 0; j < NP; ++j) {
-        const int q = h * NP + j;
-        const float4 m = meta[q];
-        const int sq = __float_as_int(m.z);
-        const int sp = sq < 0 ? cur_sp : sq;
-        if (__any_sync(0xffffffffu, sp != cur_sp)) {
+        for (int j = 0; j < NP; ++j) {
+          const int q = h * NP + j;
+          const int spq = spp[q];
+          if (__any_sync(0xffffffffu, spq != cur_sp)) {
 #pragma unroll
-          for (int hh = 0; hh < H; ++hh) {  // streams flush one after the other
-            if (h == hh && sp != cur_sp) {
-              if (cur_sp >= 0 && active) {
-                float* dst = cbuf + (cur_sp * N + n) * KC;
+            for (int hh = 0; hh < H; ++hh) {  // streams flush one after the other
+              if (h == hh && spq != cur_sp) {
+                if (cur_sp >= 0 && active) {
+                  float* dst = cbuf + (cur_sp * N + n) * KC;
 #pragma unroll
-                for (int k = 0; k < K; ++k) dst[k] += acc[k];
+                  for (int k = 0; k < K; ++k) dst[k] += acc[k];
+                }
+#pragma unroll
+                for (int k = 0; k < K; ++k) acc[k] = 0.0f;
+                cur_sp = spq;
               }
-#pragma unroll
-              for (int k = 0; k < K; ++k) acc[k] = 0.0f;
-              cur_sp = sp;
-            }
-            __syncwarp();
-          }
-        }
-        const int sq2 = __float_as_int(m.y);
-        const int seg = sq2 < 0 ? cur_seg : sq2;
-        if (seg != cur_seg) {
-          if (active) {
-#pragma unroll
-            for (int l = 0; l <= L; ++l) load_coef(a.tab_b, seg, fn_index(n, l, N), NF, cf[l]);
-          }
-          cur_seg = seg;
-        }
-        float B[L + 1];
-#pragma unroll
-        for (int l = 0; l <= L; ++l) B[l] = horner7(cf[l], m.x);
-        const float4* yr = reinterpret_cast<const float4*>(Y + q * K4 + 4 * h);
-#pragma unroll
-        for (int k4 = 0; k4 < K4 / 4; ++k4) {
-          const float4 v = yr[k4];
-          const float vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const int k = 4 * k4 + i;
-            if (k < K) {
-              int l = 0;
-              while ((l + 1) * (l + 1) <= k) ++l;  // compile time: k is unrolled
-              acc[k] = fmaf(B[l], vv[i], acc[k]);
+              __syncwarp();
             }
           }
+          if ((seg_chg >> q) & 1u) {
+            const int sq = sg[q];
+            if (active) {
+#pragma unroll
+              for (int l = 0; l <= L; ++l) load_coef(a.tab_b, sq, fn_index(n, l, N), NF, cf[l]);
+            }
+          }
+          accumulate_pair<L, K4>(acc, cf, tt[q], Y + q * K4 + 4 * h);
         }
       }
+      cur_seg = sg[h * NP + NP - 1];
+      cur_sp = spp[h * NP + NP - 1];
       __syncwarp();
     }
 #pragma unroll
