@@ -481,16 +481,19 @@ def diff_forces(soap_cls, torch, steps: int = 20, warmup: int = 3):
     for _ in range(warmup):
         step()
     torch.cuda.synchronize()
-    soap.profile = []
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(steps):
         step()
     e1.record()
     torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    # per-stage times from separate steps (the stage events add host work of their own)
+    soap.profile = []
+    for _ in range(steps):
+        step()
     st = {k: v / steps for k, v in soap.stage_times().items()}
     soap.profile = None
-    ms = e0.elapsed_time(e1) / steps
     n = len(box["atomic_numbers"])
     # the same step through the SOAP.batch graph plan (forward and adjoint replayed as graphs)
     plan = soap.batch([box])

@@ -179,15 +179,31 @@ class _Batch:
                     pbcs[i] = np.asarray(r[3].detach().cpu() if isinstance(r[3], torch.Tensor) else r[3],
                                          dtype=bool).reshape(3)
         all_atoms = all(c is None for c in centers_list)
-        # the small host arrays (and host positions) go to the device in ONE
-        # asynchronous copy from a pinned staging buffer
-        arrays = [("species", soap._species_lookup(Zall)), ("atom_off", atom_off), ("cells", cells), ("pbc", pbcs)]
-        if all_atoms:
-            arrays.append(("centre_struct", np.repeat(np.arange(len(raw), dtype=np.int32), counts_a)))
-        if host_pos:
-            host = np.concatenate([r[0] for r in raw]) if raw else np.zeros((0, 3))
-            arrays.append(("positions", np.ascontiguousarray(host, dtype=np.float64)))
-        dev_arrays = soap._upload(arrays)
+        # Structures evaluated again with new device positions (an MD or relaxation loop) reuse
+        # the device copies of their species, offsets, cells, pbc and centre indices: the
+        # atomic numbers, cells and flags are compared with the cached ones on the host.
+        cached = soap._topology if (all_atoms and not host_pos) else None
+        if cached is not None and not (cached["counts"] == counts_a and np.array_equal(cached["Z"], Zall)
+                                       and np.array_equal(cached["cells"], cells)
+                                       and np.array_equal(cached["pbcs"], pbcs)):
+            cached = None
+        if cached is not None:
+            dev_arrays = cached["dev"]
+        else:
+            # the small host arrays (and host positions) go to the device in ONE
+            # asynchronous copy from a pinned staging buffer
+            arrays = [("species", soap._species_lookup(Zall)), ("atom_off", atom_off), ("cells", cells),
+                      ("pbc", pbcs)]
+            if all_atoms:
+                arrays.append(("centre_struct", np.repeat(np.arange(len(raw), dtype=np.int32), counts_a)))
+                arrays.append(("centre_atom", np.arange(int(atom_off[-1]), dtype=np.int32)))
+            if host_pos:
+                host = np.concatenate([r[0] for r in raw]) if raw else np.zeros((0, 3))
+                arrays.append(("positions", np.ascontiguousarray(host, dtype=np.float64)))
+            dev_arrays = soap._upload(arrays)
+            if all_atoms and not host_pos:
+                soap._topology = {"counts": list(counts_a), "Z": Zall.copy(), "cells": cells.copy(),
+                                  "pbcs": pbcs.copy(), "dev": dev_arrays}
         self.species, self.atom_off = dev_arrays["species"], dev_arrays["atom_off"]
         self.cells, self.pbc = dev_arrays["cells"], dev_arrays["pbc"]
         if host_pos:
@@ -205,7 +221,7 @@ class _Batch:
             self.counts = counts_a
             self.n_centres = self.n_atoms
             self.centre_xyz = self.positions
-            self.centre_atom = torch.arange(self.n_atoms, dtype=torch.int32, device=dev)
+            self.centre_atom = dev_arrays["centre_atom"]
             self.centre_attach = self.centre_atom
             self.centre_struct = dev_arrays["centre_struct"]
         else:
@@ -527,6 +543,7 @@ class SOAP:
         self._poly_grid = _poly_grid(self._r_cut, self._n_max, self.quad_n) if self._rbf == "polynomial" else None
         self._build_basis()
         self._counter = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._topology = None  # device copies of the last batch's species, offsets, cells (see _Batch)
         self.n_features = int(self.get_number_of_features())
         # When a list, every library call appends (name, start_event, end_event)
         # recorded on the launch stream (per-stage GPU timing).
