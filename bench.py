@@ -442,8 +442,8 @@ def run_batched_only(args):
 
     def one():
         sysl = [dict(c, positions=c["positions"].clone().requires_grad_(True)) for c in dev_cells]
-        out = soap.create(sysl)
-        E = ((torch.cat(out) if isinstance(out, list) else out) @ w).sum()
+        out, _ = soap.create_flat(sysl)
+        E = (out @ w).sum()
         E.backward()
 
     one()
