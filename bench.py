@@ -748,6 +748,9 @@ def run_ours(args):
             "atoms_per_step": n_at, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk, "cpu_baseline": cpu,
             "batched_vs_plain": extra, "scale_create": scale, "diff_forces": diff, "plain_cpu_cluster192": plain192,
+            "reference_gpu_kernels": "unavailable on this box: the reference's Triton Jacobian kernels live in its "
+                                     "Python package, which does not travel to the benchmark host, and its GPU "
+                                     "path needs the sphericart CUDA library, which is not installed there",
             "parity_vs_fp64": parity}
     print(json.dumps(line), flush=True)
 

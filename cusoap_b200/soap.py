@@ -41,6 +41,9 @@ from .xyz import ATOMIC_NUMBERS as _SYMBOLS
 
 # Parameter limits of the compiled kernels (csrc/common.cuh kMaxN, kMaxL, kMaxS).
 MAX_N_MAX, MAX_L_MAX, MAX_SPECIES = 16, 9, 16
+# Per-centre (row, edge) entries the closed-form Jacobian kernel stages
+# (csrc/jacobian.cu): one per neighbour pair, two with attach=True.
+JACOBIAN_MAX_ENTRIES = 8192
 
 _F64_WARNED = False
 
@@ -891,6 +894,12 @@ class SOAP:
             mode = self._out_mode()
             F = self.get_number_of_features()
             pairs = _Pairs(self, batch, _lib.NL_ALL)
+            entries = (2 if attach else 1) * pairs.max_pairs
+            if entries > JACOBIAN_MAX_ENTRIES:
+                raise ValueError(f"derivatives: a centre has {pairs.max_pairs} neighbours within the cutoff "
+                                 f"({entries} Jacobian entries{' with attach=True' if attach else ''}); the "
+                                 f"closed-form Jacobian kernel stages at most {JACOBIAN_MAX_ENTRIES} per centre. "
+                                 f"Use a smaller r_cut or the adjoint (create() with positions requiring grad).")
             desc, coeff = self._run_descriptor(batch, pairs, mode, want_coeff=True)
             deriv = torch.empty((batch.n_centres, n_inc, 3, F), dtype=torch.float32, device=self.device)
             if n_inc > 0 and batch.n_centres > 0:

@@ -172,3 +172,20 @@ def test_forces_status_word_is_clear_after_an_adjoint():
     s.create(dict(box, positions=pos)).sum().backward()
     assert s.forces_status() == 0
     assert torch.isfinite(pos.grad).all()
+
+
+def test_jacobian_entry_limit_is_a_clear_error():
+    """More neighbours per centre than the closed-form Jacobian kernel stages
+    (JACOBIAN_MAX_ENTRIES; half that with attach=True) is refused before any
+    Jacobian work, naming the limit; the adjoint path has no such limit."""
+    from cusoap_b200 import SOAP
+    from cusoap_b200.soap import JACOBIAN_MAX_ENTRIES
+    sysd = W.water_cluster(14, 14, 14, seed=1)  # 8232 atoms, every one within the cutoff of atom 0
+    s = SOAP(species=[1, 8], r_cut=100.0, n_max=2, l_max=1, sigma=0.5)
+    with pytest.raises(ValueError, match=str(JACOBIAN_MAX_ENTRIES)):
+        s.derivatives(sysd, centers=[0], include=[0])
+    small = W.water_cluster(12, 12, 12, seed=1)  # 5184 atoms: fits without attach, not with it
+    J = s.derivatives(small, centers=[0], include=[0, 1], return_descriptor=False)
+    assert J.shape == (1, 2, 3, s.get_number_of_features()) and torch.isfinite(J).all()
+    with pytest.raises(ValueError, match="attach"):
+        s.derivatives(small, centers=[0], include=[0], attach=True)
