@@ -369,6 +369,80 @@ __global__ void __launch_bounds__(128, 4) k_descriptor_2s(DescArgs a) {
   descriptor_body<L, GN, 2>(a);
 }
 
+// Epilogue of the radial-index-lane kernel: coefficient rows KR = K4 floats
+// apart (16-byte aligned).  For the power spectrum each lane takes one (n, n')
+// pair of a species block and walks every l with compile-time m loops,
+// reading the two rows as float4; for each l the lanes write consecutive
+// features (coalesced).  Same outputs and DScribe order as desc_epilogue.
+template <int L, int KR>
+__device__ __forceinline__ void desc_epilogue_n(const DescArgs& a, int64_t c, const float* cbuf, int lane,
+                                                const float* s_pref, const int* s_blk, const unsigned char* s_tri) {
+  constexpr int K = (L + 1) * (L + 1);
+  const int N = a.N, S = a.S;
+  if (a.coeff_out) {
+    float* crow = a.coeff_out + (size_t)c * S * N * K;
+    for (int f = lane; f < S * N * K; f += 32) {
+      const int sn = f / K;
+      crow[f] = cbuf[sn * KR + (f - sn * K)];
+    }
+  }
+  float* orow = a.out + (size_t)c * a.F;
+  if (a.mode != SOAPB_OUT_PS) {
+    const bool cc = a.mode == SOAPB_OUT_CC;
+    const float pi_m15 = (float)(1.0 / (kPi * 1.7724538509055160273));  // pi^-3/2
+    for (int f = lane; f < a.F; f += 32) {
+      const int sn = f / K, lm = f - sn * K;
+      int src = lm;
+      float scale = 1.0f;
+      if (cc) {
+        // l = 1 stored (z, x, y) = source lm (2, 3, 1); lm >= 4 scaled by pi^-3/2
+        if (lm >= 1 && lm <= 3) src = (lm == 3) ? 1 : lm + 1;
+        if (lm >= 4) scale = pi_m15;
+      }
+      orow[f] = cbuf[sn * KR + src] * scale;
+    }
+    return;
+  }
+  const int nblk = a.crossover ? S * (S + 1) / 2 : S;
+  for (int b = 0; b < nblk; ++b) {
+    const int jj = s_blk[2 * b], fb0 = s_blk[2 * b + 1];
+    const int j = jj & 255, jd = jj >> 8;
+    const bool diag = j == jd;
+    const int np = diag ? N * (N + 1) / 2 : N * N;
+    for (int p = lane; p < np; p += 32) {
+      int n, nd;
+      if (diag) {
+        n = s_tri[2 * p];
+        nd = s_tri[2 * p + 1];
+      } else {
+        n = p / N;
+        nd = p - n * N;
+      }
+      const float4* x4 = reinterpret_cast<const float4*>(cbuf + (j * N + n) * KR);
+      const float4* y4 = reinterpret_cast<const float4*>(cbuf + (jd * N + nd) * KR);
+      float* o = orow + fb0 + p;
+#pragma unroll
+      for (int l = 0; l <= L; ++l) {
+        const int q0 = (l * l) / 4, q1 = ((l + 1) * (l + 1) - 1) / 4;  // float4 chunks holding slots l^2..(l+1)^2-1
+        float xv[16], yv[16];
+#pragma unroll
+        for (int q = q0; q <= q1; ++q) {
+          const float4 u = x4[q], v = y4[q];
+          xv[4 * (q - q0)] = u.x; xv[4 * (q - q0) + 1] = u.y; xv[4 * (q - q0) + 2] = u.z; xv[4 * (q - q0) + 3] = u.w;
+          yv[4 * (q - q0)] = v.x; yv[4 * (q - q0) + 1] = v.y; yv[4 * (q - q0) + 2] = v.z; yv[4 * (q - q0) + 3] = v.w;
+        }
+        float acc = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 2 * l + 1; ++m) {
+          const int i = l * l + m - 4 * q0;
+          acc = fmaf(xv[i], yv[i], acc);
+        }
+        o[l * np] = acc * s_pref[l];
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Radial-index lanes (n_max <= 8, l_max <= 6): lane n of a stream owns the
 // radial index n and ALL K = (l_max+1)^2 accumulators c[n][lm] of it, so
@@ -394,7 +468,10 @@ struct NShape {
   static constexpr int K = (L + 1) * (L + 1);
   static constexpr int K4 = (K + 3) & ~3;  // row length in floats: float4 reads and writes
   static constexpr int H = 32 / NP;
-  static constexpr int KC = K | 1;
+  // coefficient rows c[s][n][0..K) also K4 floats apart: 16-byte aligned for the epilogue's
+  // float4 reads, and the 8 rows n of a species (K4 = 4, 12, 16, 28, 36 or 52) start on 8
+  // different groups of four banks
+  static constexpr int KC = K4;
   // row q = h NP + j starts at q K4 + 4 h: the H streams' float4 reads of the
   // same slot fall on different groups of four banks whatever K4 is
   static constexpr int YF = 32 * K4 + 4 * H;
@@ -573,7 +650,7 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
       }
       __syncwarp();
     }
-    desc_epilogue<L>(a, c, cbuf, lane, s_pref, s_blk, s_tri);
+    desc_epilogue_n<L, KC>(a, c, cbuf, lane, s_pref, s_blk, s_tri);
     __syncwarp();
   }
 }
