@@ -554,7 +554,8 @@ def scale_create(soap_cls, torch, steps: int = 3, warmup: int = 2, n_mol: int = 
     n_pairs = _Pairs(soap, _Batch(soap, [system], [None]), _lib.NL_CREATE).total
     N, L = W.CONFIGS["cluster1M"]["n_max"], W.CONFIGS["cluster1M"]["l_max"]
     K = (L + 1) ** 2
-    flop = n_pairs * (2 * N * K + N * (L + 1) * 16) + n_at * 2 * F * K / (L + 1)
+    # a degree-7 Horner pass is 7 FMAs = 14 FLOP per radial function and pair
+    flop = n_pairs * (2 * N * K + N * (L + 1) * 14) + n_at * 2 * F * K / (L + 1)
     byts = n_pairs * 16 + n_at * F * 4
     d_ms = st.get("descriptor", float("nan"))
     peak, _ = _peaks()
@@ -565,7 +566,7 @@ def scale_create(soap_cls, torch, steps: int = 3, warmup: int = 2, n_mol: int = 
             "descriptor": {"hbm_bytes": byts, "gbs": byts / d_ms / 1e6, "hbm_frac_of_measured": byts / d_ms / 1e6 / peak,
                            "flop": flop, "tflops": flop / d_ms / 1e9,
                            "fp32_frac_of_nominal": flop / d_ms / 1e9 / FP32_PEAK_TFLOPS,
-                           "note": "flop = pairs x (2 N K accumulate + 16 N (l_max+1) radial Horner) + centres x "
+                           "note": "flop = pairs x (2 N K accumulate + 14 N (l_max+1) radial Horner, 7 FMAs per function) + centres x "
                                    "2 F K/(l_max+1) power spectrum; bytes = 16 B per pair read + F x 4 B per row"}}
 
 

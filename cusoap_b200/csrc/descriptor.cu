@@ -506,6 +506,22 @@ __device__ __forceinline__ void accumulate_pair(float (&acc)[(L + 1) * (L + 1)],
   }
 }
 
+// Adds a lane's K accumulators to its 16-byte-aligned coefficient row (float4
+// read-modify-write; the row's K4 - K padding slots stay zero).
+template <int K, int K4>
+__device__ __forceinline__ void flush_row(float* row, const float (&acc)[K]) {
+  float4* r4 = reinterpret_cast<float4*>(row);
+#pragma unroll
+  for (int q = 0; q < K4 / 4; ++q) {
+    float4 v = r4[q];
+    v.x += acc[4 * q];
+    if (4 * q + 1 < K) v.y += acc[4 * q + 1];
+    if (4 * q + 2 < K) v.z += acc[4 * q + 2];
+    if (4 * q + 3 < K) v.w += acc[4 * q + 3];
+    r4[q] = v;
+  }
+}
+
 template <int L, int NP>
 __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
   using Sh = NShape<L, NP>;
@@ -533,7 +549,7 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
     if (lane == 0) c32 = atomicAdd(a.counter, 1);
     const int64_t c = __shfl_sync(0xffffffffu, c32, 0);
     if (c >= a.n_centres) break;
-    for (int i = lane; i < cbn; i += 32) cbuf[i] = 0.0f;
+    for (int i = lane; i < cbn / 4; i += 32) reinterpret_cast<float4*>(cbuf)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     const int64_t p0 = a.pair_off[c], P = a.pair_off[c + 1] - p0;
     const int64_t s0 = p0 + (P * h) / H, s1 = p0 + (P * (h + 1)) / H;  // this stream's pairs
     const int64_t rounds = (P + H - 1) / H;                             // longest stream
@@ -556,17 +572,23 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
       int seg = -1, sp = -1;
       float t = 0.0f;
       {
+        // a row past the end of this stream is the harmonics of the origin, (Y00, 0, ..., 0),
+        // with R_00 scaled to 0: a zero row that adds nothing
         float yv[K4];
 #pragma unroll
-        for (int k = 0; k < K4; ++k) yv[k] = 0.0f;
-        if (valid) {
-          const float4 pr = __ldg(a.pairs + e);
-          const float r = sqrtf(pr.x * pr.x + pr.y * pr.y + pr.z * pr.z);
-          seg_coord(r, a.inv_h, a.nseg, seg, t);
-          sp = (int)((unsigned)__float_as_int(pr.w) >> kAtomBits);
-          SolidHarmonics<L>::values(pr.x, pr.y, pr.z, [&](int idx, float v) { yv[idx] = v; });
-          if (!(r > 0.0f)) yv[0] *= a.self_ratio;  // the centre's own Gaussian: w0 B_n0(0) Y00
-        }  // past the end of this stream: a zero row that adds nothing
+        for (int k = K; k < K4; ++k) yv[k] = 0.0f;
+        const float4 pr = valid ? __ldg(a.pairs + e) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float r = sqrtf(pr.x * pr.x + pr.y * pr.y + pr.z * pr.z);
+        seg_coord(r, a.inv_h, a.nseg, seg, t);
+        sp = (int)((unsigned)__float_as_int(pr.w) >> kAtomBits);
+        SolidHarmonics<L>::values(pr.x, pr.y, pr.z, [&](int idx, float v) { yv[idx] = v; });
+        // the centre's own Gaussian (r = 0): w0 B_n0(0) Y00
+        yv[0] *= valid ? ((r > 0.0f) ? 1.0f : a.self_ratio) : 0.0f;
+        if (!valid) {
+          seg = -1;
+          sp = -1;
+          t = 0.0f;
+        }
 #pragma unroll
         for (int k4 = 0; k4 < K4 / 4; ++k4)
           myrow[k4] = make_float4(yv[4 * k4], yv[4 * k4 + 1], yv[4 * k4 + 2], yv[4 * k4 + 3]);
@@ -616,9 +638,7 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
             for (int hh = 0; hh < H; ++hh) {  // streams flush one after the other
               if (h == hh && spq != cur_sp) {
                 if (cur_sp >= 0 && active) {
-                  float* dst = cbuf + (cur_sp * N + n) * KC;
-#pragma unroll
-                  for (int k = 0; k < K; ++k) dst[k] += acc[k];
+                  flush_row<K, K4>(cbuf + (cur_sp * N + n) * KC, acc);
                 }
 #pragma unroll
                 for (int k = 0; k < K; ++k) acc[k] = 0.0f;
@@ -644,9 +664,7 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
 #pragma unroll
     for (int hh = 0; hh < H; ++hh) {
       if (h == hh && cur_sp >= 0 && active) {
-        float* dst = cbuf + (cur_sp * N + n) * KC;
-#pragma unroll
-        for (int k = 0; k < K; ++k) dst[k] += acc[k];
+        flush_row<K, K4>(cbuf + (cur_sp * N + n) * KC, acc);
       }
       __syncwarp();
     }
