@@ -430,12 +430,19 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
         float xi[2 * L + 1], ze[2 * L + 1];
 #pragma unroll
         for (int m = 0; m < 2 * l + 1; ++m) { xi[m] = 0.0f; ze[m] = 0.0f; }
+        // function-major table: row fn = l N + n, column seg.  The next function's two
+        // float4 loads are issued before this one is evaluated, so their latency overlaps
+        // the Horner pass and the G contraction.
+        float cf[kNCoef];
+        load_coef(a.tabf, l * N, seg, nsegf, cf);
+#pragma unroll 2
         for (int n = 0; n < N; ++n) {
-          const int fn = l * N + n;
-          float cf[kNCoef];
-          load_coef(a.tabf, fn, seg, nsegf, cf);  // function-major: row fn, column seg
+          float nx[kNCoef];
+          load_coef(a.tabf, l * N + min(n + 1, N - 1), seg, nsegf, nx);
           float p, dp;
           horner7_d(cf, t, p, dp);
+#pragma unroll
+          for (int k = 0; k < kNCoef; ++k) cf[k] = nx[k];
           // an r = 0 edge adds nothing: its l = 0 term has no gradient and
           // B_nl(0) = 0 for l >= 1, so b = 0 there (and h = 0 through dt_r)
           const float b = self_edge ? 0.0f : p, h = dp * dt_r;
