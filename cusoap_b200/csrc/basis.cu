@@ -414,6 +414,8 @@ extern "C" int soapb_basis_plan(soapb_basis* b) {
   if (!b) return set_error(SOAPB_ERR_ARG, "null basis");
   if (b->n_max < 1 || b->n_max > kMaxN) return set_error(SOAPB_ERR_ARG, "n_max must be in [1, %d]", kMaxN);
   if (b->l_max < 0 || b->l_max > kMaxL) return set_error(SOAPB_ERR_ARG, "l_max must be in [0, %d]", kMaxL);
+  if (b->l_max >= 10 && b->n_max > 8)
+    return set_error(SOAPB_ERR_ARG, "l_max >= 10 is built for n_max <= 8 (got n_max %d)", b->n_max);
   if (b->n_species < 1 || b->n_species > kMaxS)
     return set_error(SOAPB_ERR_ARG, "n_species must be in [1, %d]", kMaxS);
   if (!(b->r_cut > 0.0) || !(b->sigma > 0.0)) return set_error(SOAPB_ERR_ARG, "r_cut and sigma must be > 0");

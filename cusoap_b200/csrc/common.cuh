@@ -10,7 +10,7 @@ namespace soapb {
 
 constexpr int kDeg = 7;              // radial table: degree-7 polynomial per segment
 constexpr int kNCoef = kDeg + 1;
-constexpr int kMaxL = 9;
+constexpr int kMaxL = 12;
 constexpr int kMaxN = 16;
 constexpr int kMaxS = 16;
 constexpr int kMaxKeys = 1024;       // species x radial segments (neighbour sort keys)
@@ -216,6 +216,9 @@ inline int dispatch_l(int l, Args&&... args) {
     case 7: return F<7>::run(args...);
     case 8: return F<8>::run(args...);
     case 9: return F<9>::run(args...);
+    case 10: return F<10>::run(args...);
+    case 11: return F<11>::run(args...);
+    case 12: return F<12>::run(args...);
     default: return set_error(SOAPB_ERR_UNSUPPORTED, "l_max %d > %d not built", l, kMaxL);
   }
 }

@@ -43,11 +43,12 @@ struct DescArgs {
 // Position of harmonic block l in a pair's Y row: l^2 plus a padding that
 // starts every block on a different shared-memory bank (the lane groups of the
 // l blocks read the same slot m of their blocks at once: no conflicts).  Plain
-// l^2 puts l = 6 on the bank of l = 2 (36 = 4 mod 32) and l = 8 on that of
-// l = 0; one float of padding from l = 6 and another from l = 8 separate them.
-__host__ __device__ constexpr int ybase(int l) { return l * l + (l >= 6) + (l >= 8); }
-// Y row position of harmonic index idx = l^2 + l + m (idx >= 36 is l >= 6, idx >= 64 is l >= 8).
-__host__ __device__ constexpr int ypos(int idx) { return idx + (idx >= 36) + (idx >= 64); }
+// l^2 puts l = 6 on the bank of l = 2 (36 = 4 mod 32), l = 8 on that of l = 0
+// and l = 12 on that of l = 4; one float of padding from l = 6, another from
+// l = 8 and two more from l = 12 separate them (checked below).
+__host__ __device__ constexpr int ybase(int l) { return l * l + (l >= 6) + (l >= 8) + 2 * (l >= 12); }
+// Y row position of harmonic index idx = l^2 + l + m (idx >= 36: l >= 6, >= 64: l >= 8, >= 144: l >= 12).
+__host__ __device__ constexpr int ypos(int idx) { return idx + (idx >= 36) + (idx >= 64) + 2 * (idx >= 144); }
 
 constexpr bool ybase_banks_distinct() {
   for (int l = 0; l <= kMaxL; ++l) {
@@ -747,13 +748,18 @@ struct DescDispatch {
         }
       }
     }
-    switch (gn) {
-      case 1: return launch_descriptor<L, 1, 1>(a, wpb, st);
-      case 2: return launch_descriptor<L, 2, 1>(a, wpb, st);
-      case 3: return launch_descriptor<L, 3, 1>(a, wpb, st);
-      case 4: return launch_descriptor<L, 4, 1>(a, wpb, st);
-      case 6: return launch_descriptor<L, 6, 1>(a, wpb, st);
-      default: return set_error(SOAPB_ERR_UNSUPPORTED, "descriptor: %d radial functions per lane not built", gn);
+    if constexpr (L >= 10) {  // two lanes per l: 4 radial functions per lane cover n_max <= 8
+      if (a.N > 8) return set_error(SOAPB_ERR_UNSUPPORTED, "descriptor: l_max %d is built for n_max <= 8", L);
+      return launch_descriptor<L, 4, 1>(a, wpb, st);
+    } else {
+      switch (gn) {
+        case 1: return launch_descriptor<L, 1, 1>(a, wpb, st);
+        case 2: return launch_descriptor<L, 2, 1>(a, wpb, st);
+        case 3: return launch_descriptor<L, 3, 1>(a, wpb, st);
+        case 4: return launch_descriptor<L, 4, 1>(a, wpb, st);
+        case 6: return launch_descriptor<L, 6, 1>(a, wpb, st);
+        default: return set_error(SOAPB_ERR_UNSUPPORTED, "descriptor: %d radial functions per lane not built", gn);
+      }
     }
   }
 };

@@ -40,7 +40,9 @@ from .xyz import ATOMIC_NUMBERS as _SYMBOLS
 
 
 # Parameter limits of the compiled kernels (csrc/common.cuh kMaxN, kMaxL, kMaxS).
-MAX_N_MAX, MAX_L_MAX, MAX_SPECIES = 16, 9, 16
+MAX_N_MAX, MAX_L_MAX, MAX_SPECIES = 16, 12, 16
+# l_max 10-12 are built for n_max up to 8 (two lanes per l, four radial functions per lane)
+MAX_N_MAX_HIGH_L = 8
 # Per-centre (row, edge) entries the closed-form Jacobian kernel stages
 # (csrc/jacobian.cu): one per neighbour pair, two with attach=True.
 JACOBIAN_MAX_ENTRIES = 8192
@@ -507,6 +509,9 @@ class SOAP:
         if not 0 <= self._l_max <= MAX_L_MAX:
             raise ValueError(f"l_max must be in [0, {MAX_L_MAX}] (the CUDA kernels are built up to l_max "
                              f"{MAX_L_MAX}); got {self._l_max}")
+        if self._l_max >= 10 and self._n_max > MAX_N_MAX_HIGH_L:
+            raise ValueError(f"n_max must be <= {MAX_N_MAX_HIGH_L} for l_max >= 10 (the CUDA kernels are built "
+                             f"for that); got n_max {self._n_max}, l_max {self._l_max}")
         if self.n_species > MAX_SPECIES:
             raise ValueError(f"at most {MAX_SPECIES} species are supported (the CUDA kernels are built up to "
                              f"{MAX_SPECIES}); got {self.n_species}")

@@ -40,22 +40,29 @@ def test_empty_centres_and_empty_structure_in_a_batch():
     assert _row_err(outs[2].cpu().numpy(), o.create(one["positions"], one["atomic_numbers"])) < DESC_TOL
 
 
-def test_largest_l_max_create_derivatives_forces():
+@pytest.mark.parametrize("n_max,l_max,periodic", [(10, 9, False), (8, 10, False), (6, 12, False), (5, 12, True)])
+def test_large_l_max_create_derivatives_forces(n_max, l_max, periodic):
+    """l_max 9 (the largest of the lanes-grouped-by-l launch shapes with
+    n_max up to 16) and l_max 10-12 (one launch shape, n_max <= 8): create,
+    the closed-form Jacobian and adjoint forces against the FP64 oracle."""
     from cusoap_b200 import SOAP
-    P = dict(species=[1, 8], r_cut=4.0, n_max=10, l_max=9, sigma=0.5)
+    P = dict(species=[1, 8], r_cut=4.0, n_max=n_max, l_max=l_max, sigma=0.5, periodic=periodic)
     s = SOAP(**P)
     o = OracleSOAP(**P)
     sysd = W.water_cluster(2, 2, 2, seed=6)
+    if periodic:
+        sysd = dict(sysd, cell=np.eye(3) * 7.2, pbc=[True, True, True])
     pos, Z = sysd["positions"], sysd["atomic_numbers"]
-    assert _row_err(s.create(sysd).cpu().numpy(), o.create(pos, Z)) < DESC_TOL
-    J = s.derivatives(sysd, centers=[0, 5], include=list(range(10)), return_descriptor=False)
-    Jo = o.derivatives(pos, Z, centers=[0, 5], include=list(range(10)), return_descriptor=False)
-    assert _row_err(J.cpu().numpy(), Jo) < DERIV_TOL
+    cell, pbc = sysd.get("cell"), sysd.get("pbc")
+    assert _row_err(s.create(sysd).cpu().numpy(), o.create(pos, Z, cell=cell, pbc=pbc)) < DESC_TOL
+    if not periodic:  # the oracle's closed-form Jacobian is the non-periodic one (SG:2270-2626)
+        J = s.derivatives(sysd, centers=[0, 5], include=list(range(10)), return_descriptor=False)
+        Jo = o.derivatives(pos, Z, centers=[0, 5], include=list(range(10)), return_descriptor=False)
+        assert _row_err(J.cpu().numpy(), Jo) < DERIV_TOL
     w = np.random.default_rng(0).standard_normal(s.get_number_of_features())
     pt = torch.tensor(pos, device="cuda", requires_grad=True)
-    (s.create({"positions": pt, "atomic_numbers": Z}) * torch.tensor(w, dtype=torch.float32,
-                                                                     device="cuda")).sum().backward()
-    Fo = o.forces(pos, Z, np.tile(w, (len(Z), 1)))
+    (s.create(dict(sysd, positions=pt)) * torch.tensor(w, dtype=torch.float32, device="cuda")).sum().backward()
+    Fo = o.forces(pos, Z, np.tile(w, (len(Z), 1)), cell, pbc)
     assert rel_l2(-pt.grad.cpu().numpy(), Fo) < DERIV_TOL
 
 

@@ -48,7 +48,7 @@ def test_basis_plan_matches_oracle(name):
 def test_basis_plan_rejects_bad_sizes():
     lib = _lib.load()
     b = _lib.Basis()
-    b.n_max, b.l_max, b.n_species, b.crossover, b.r_cut, b.sigma = 4, 12, 1, 1, 5.0, 0.5
+    b.n_max, b.l_max, b.n_species, b.crossover, b.r_cut, b.sigma = 4, 13, 1, 1, 5.0, 0.5
     st = lib.soapb_basis_plan(ctypes.byref(b))
     assert st == _lib.ERR_ARG
     assert "l_max" in lib.soapb_last_error().decode()
@@ -72,9 +72,9 @@ def test_soap_requires_cuda_device():
 
 
 def test_soap_refuses_sizes_beyond_the_kernels_before_device_work():
-    """The kernels are built up to n_max 16, l_max 9 and 16 species; larger
-    requests raise ValueError naming the limit, before any CUDA call (this
-    runs without a GPU, and device=None would need one)."""
+    """The kernels are built up to n_max 16, l_max 12 (n_max 8 from l_max 10)
+    and 16 species; larger requests raise ValueError naming the limit, before
+    any CUDA call (this runs without a GPU, and device=None would need one)."""
     from cusoap_b200 import SOAP
     from cusoap_b200.soap import MAX_L_MAX, MAX_N_MAX, MAX_SPECIES
     with pytest.raises(ValueError, match="l_max must be in"):
@@ -83,11 +83,17 @@ def test_soap_refuses_sizes_beyond_the_kernels_before_device_work():
         SOAP(species=[1, 8], r_cut=5.0, n_max=MAX_N_MAX + 1, l_max=3)
     with pytest.raises(ValueError, match="species"):
         SOAP(species=list(range(1, MAX_SPECIES + 2)), r_cut=5.0, n_max=4, l_max=3)
+    with pytest.raises(ValueError, match="l_max >= 10"):
+        SOAP(species=[1, 8], r_cut=5.0, n_max=9, l_max=10)
     # the Python limits are the library's
     lib = _lib.load()
     b = _lib.Basis()
-    b.n_max, b.l_max, b.n_species, b.crossover, b.r_cut, b.sigma = MAX_N_MAX, MAX_L_MAX, MAX_SPECIES, 1, 5.0, 0.5
+    b.n_max, b.l_max, b.n_species, b.crossover, b.r_cut, b.sigma = 8, MAX_L_MAX, MAX_SPECIES, 1, 5.0, 0.5
     assert lib.soapb_basis_plan(ctypes.byref(b)) == _lib.OK
+    b.n_max, b.l_max = MAX_N_MAX, 9
+    assert lib.soapb_basis_plan(ctypes.byref(b)) == _lib.OK
+    b.n_max, b.l_max = 9, 10
+    assert lib.soapb_basis_plan(ctypes.byref(b)) == _lib.ERR_ARG
     for field, value in (("n_max", MAX_N_MAX + 1), ("l_max", MAX_L_MAX + 1), ("n_species", MAX_SPECIES + 1)):
         c = _lib.Basis()
         c.n_max, c.l_max, c.n_species, c.crossover, c.r_cut, c.sigma = 4, 3, 2, 1, 5.0, 0.5
