@@ -551,9 +551,12 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
     const int64_t c = __shfl_sync(0xffffffffu, c32, 0);
     if (c >= a.n_centres) break;
     for (int i = lane; i < cbn / 4; i += 32) reinterpret_cast<float4*>(cbuf)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    const int64_t p0 = a.pair_off[c], P = a.pair_off[c + 1] - p0;
-    const int64_t s0 = p0 + (P * h) / H, s1 = p0 + (P * (h + 1)) / H;  // this stream's pairs
-    const int64_t rounds = (P + H - 1) / H;                             // longest stream
+    // offsets inside the centre's list are 32-bit: 2^31 pairs of one centre would be 34 GB of list
+    const int64_t p0 = a.pair_off[c];
+    const int P = (int)(a.pair_off[c + 1] - p0);
+    const float4* pc = a.pairs + p0;
+    const int s0 = (int)(((int64_t)P * h) / H), s1 = (int)(((int64_t)P * (h + 1)) / H);  // this stream's pairs
+    const int rounds = (P + H - 1) / H;                                                  // longest stream
     float acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = 0.0f;
@@ -562,14 +565,17 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
     for (int l = 0; l <= L; ++l)
 #pragma unroll
       for (int k = 0; k < kNCoef; ++k) cf[l][k] = 0.0f;
-    int cur_sp = -1, cur_seg = -1;
+    // each stream starts on the species of its first pair, so the centre's first batch takes the
+    // fast path unless a species changes inside it
+    int cur_sp = (s0 < s1) ? (int)((unsigned)__float_as_int(__ldg(&pc[s0].w)) >> kAtomBits) : -1;
+    int cur_seg = -1;
     __syncwarp();
 
-    for (int64_t base = 0; base < rounds; base += NP) {
+    for (int base = 0; base < rounds; base += NP) {
       // stage: lane (h, n) takes pair s0 + base + n of its stream into row `lane`
-      const int64_t e = s0 + base + n;
+      const int e = s0 + base + n;
       const bool valid = e < s1;
-      const int nvalid = (int)max((int64_t)0, min((int64_t)NP, s1 - (s0 + base)));  // this stream's block
+      const int nvalid = max(0, min(NP, s1 - (s0 + base)));  // this stream's block
       int seg = -1, sp = -1;
       float t = 0.0f;
       {
@@ -578,7 +584,9 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
         float yv[K4];
 #pragma unroll
         for (int k = K; k < K4; ++k) yv[k] = 0.0f;
-        const float4 pr = valid ? __ldg(a.pairs + e) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float4 pr = valid ? __ldg(pc + e) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        // the stream's pair of the next batch: into L1 while this batch runs
+        if (e + NP < s1) asm volatile("prefetch.global.L1 [%0];" ::"l"(pc + e + NP));
         const float r = sqrtf(pr.x * pr.x + pr.y * pr.y + pr.z * pr.z);
         seg_coord(r, a.inv_h, a.nseg, seg, t);
         sp = (int)((unsigned)__float_as_int(pr.w) >> kAtomBits);
@@ -674,8 +682,10 @@ __device__ __forceinline__ void descriptor_n_body(const DescArgs& a) {
   }
 }
 
+// l_max <= 4: 4 blocks of 4 warps per SM at 128 registers; l_max 5: 3 blocks; l_max 6: 2 blocks,
+// so its 49 accumulators and 7 x 8 coefficients per lane stay in registers (at 3 blocks they spill)
 template <int L, int NP>
-__global__ void __launch_bounds__(128, (L <= 4) ? 4 : 3) k_descriptor_n(DescArgs a) {
+__global__ void __launch_bounds__(128, (L <= 4) ? 4 : (L == 5 ? 3 : 2)) k_descriptor_n(DescArgs a) {
   descriptor_n_body<L, NP>(a);
 }
 
