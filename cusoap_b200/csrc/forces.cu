@@ -387,13 +387,15 @@ struct ForceShape {
   __host__ __device__ static int warp_floats(int S, int N) { return (S * N * KC + 3) & ~3; }
 };
 
-template <int L>
+// NT = 8: n_max 8 at compile time, so the radial loop unrolls fully and the G
+// and table offsets are immediates; NT = 0 takes n_max from the arguments.
+template <int L, int NT>
 __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
   using Sh = ForceShape<L>;
   constexpr int K = Sh::K, KC = Sh::KC;
   extern __shared__ __align__(16) float sm[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int N = a.N, SN = a.S * N, nsegf = a.nsegf;
+  const int N = (NT > 0) ? NT : a.N, SN = a.S * N, nsegf = a.nsegf;
   float* G = sm + (size_t)wid * Sh::warp_floats(a.S, N);
 
   for (;;) {
@@ -435,7 +437,7 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
         // the Horner pass and the G contraction.
         float cf[kNCoef];
         load_coef(a.tabf, l * N, seg, nsegf, cf);
-#pragma unroll 2
+#pragma unroll (NT > 0 ? NT : 2)
         for (int n = 0; n < N; ++n) {
           float nx[kNCoef];
           load_coef(a.tabf, l * N + min(n + 1, N - 1), seg, nsegf, nx);
@@ -565,7 +567,7 @@ struct ForceDispatch {
       if ((rc = check_launch("k_adjoint_g"))) return rc;
     }
     // edges
-    auto kern = k_forces<L>;
+    auto kern = (a.N == 8) ? k_forces<L, 8> : k_forces<L, 0>;
     const int per_warp = 4 * ForceShape<L>::warp_floats(a.S, a.N);
     int wpb = (wpb_tuned == 1 || wpb_tuned == 2 || wpb_tuned == 4) ? wpb_tuned : 4;
     while (wpb > 1 && wpb * per_warp > 200 * 1024) wpb >>= 1;
