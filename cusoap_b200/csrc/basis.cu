@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(512) k_basis_build(BasisDev a) {
       double d;
       exact_BD(a, s_gamma, s_pref, fn, r, f[j], d);
     }
-    cheb_to_mono(f, a.tabf + ((size_t)fn * 2 * a.nseg + seg) * kNCoef);
+    cheb_to_mono(f, a.tabf + ((size_t)fn * force_tab_stride(a.nseg) + seg) * kNCoef);
   }
   // self values: the centre's own Gaussian, w0 B_nl(0) (SG:765-819)
   for (int fn = tid; fn < NF; fn += blockDim.x) {
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(512) k_basis_build(BasisDev a) {
       }
     } else {  // the force table: value, and derivative d/dr = (4 / h) d/dt
       const int sf = seg - a.nseg;
-      const float* cf = a.tabf + ((size_t)fn * 2 * a.nseg + sf) * kNCoef;
+      const float* cf = a.tabf + ((size_t)fn * force_tab_stride(a.nseg) + sf) * kNCoef;
       for (int j = 0; j <= 16; ++j) {
         const double t = -1.0 + j / 8.0;
         const double r = (sf + 0.5 * (t + 1.0)) * (0.5 * a.h);
@@ -467,7 +467,7 @@ extern "C" int soapb_basis_plan(soapb_basis* b) {
   b->off_ftab = off; off = align_up(off + 4 * (int64_t)b->n_feat_ps, 256);
   b->off_widx = off; off = align_up(off + 4 * (int64_t)(L + 1) * (S * N) * (S * N), 256);
   b->off_err = off; off = align_up(off + 16, 256);
-  b->off_tabf = off; off = align_up(off + 4 * (int64_t)2 * b->n_seg * NF * kNCoef, 256);
+  b->off_tabf = off; off = align_up(off + 4 * (int64_t)force_tab_stride(b->n_seg) * NF * kNCoef, 256);
   b->off_self = off; off = align_up(off + 4 * (int64_t)NF, 256);
   b->off_poly = off;
   if (b->rbf == SOAPB_RBF_POLY) off = align_up(off + 8 * (int64_t)(2 + N) * b->quad_n, 256);

@@ -10,6 +10,12 @@ namespace soapb {
 
 constexpr int kDeg = 7;              // radial table: degree-7 polynomial per segment
 constexpr int kNCoef = kDeg + 1;
+// Function stride of the force table, in half-width segments: 64 when the 2 n_seg half
+// segments fit (the edge kernel's table offsets are then compile-time constants), else 2 n_seg.
+constexpr int kForceSegStride = 64;
+__host__ __device__ inline int force_tab_stride(int nseg) {
+  return 2 * nseg <= kForceSegStride ? kForceSegStride : 2 * nseg;
+}
 constexpr int kMaxL = 12;
 constexpr int kMaxN = 16;
 constexpr int kMaxS = 16;

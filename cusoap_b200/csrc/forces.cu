@@ -53,6 +53,7 @@ struct ForceArgs {
   int* status;           // bit 0: a TMA row copy of the G stage timed out (G rows NaN)
   int64_t n_centres;
   int N, S, nsegf, F, attach, crossover;
+  int fstride;   // function stride of tabf in half-width segments (force_tab_stride)
   float inv_hf;  // 1 / width of a force-table segment
 };
 
@@ -387,15 +388,16 @@ struct ForceShape {
   __host__ __device__ static int warp_floats(int S, int N) { return (S * N * KC + 3) & ~3; }
 };
 
-// NT = 8: n_max 8 at compile time, so the radial loop unrolls fully and the G
-// and table offsets are immediates; NT = 0 takes n_max from the arguments.
-template <int L, int NT>
+// FAST: n_max 8 and the table stride kForceSegStride at compile time, so the radial loop
+// unrolls fully and every G and table offset is an immediate; else both come from the arguments.
+template <int L, bool FAST>
 __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
   using Sh = ForceShape<L>;
   constexpr int K = Sh::K, KC = Sh::KC;
   extern __shared__ __align__(16) float sm[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int N = (NT > 0) ? NT : a.N, SN = a.S * N, nsegf = a.nsegf;
+  const int N = FAST ? 8 : a.N, SN = a.S * N, nsegf = a.nsegf;
+  const int fstride = FAST ? kForceSegStride : a.fstride;
   float* G = sm + (size_t)wid * Sh::warp_floats(a.S, N);
 
   for (;;) {
@@ -436,24 +438,22 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
         // float4 loads are issued before this one is evaluated, so their latency overlaps
         // the Horner pass and the G contraction.
         float cf[kNCoef];
-        load_coef(a.tabf, l * N, seg, nsegf, cf);
-#pragma unroll (NT > 0 ? NT : 2)
+        load_coef(a.tabf, l * N, seg, fstride, cf);
+#pragma unroll (FAST ? 8 : 2)
         for (int n = 0; n < N; ++n) {
           float nx[kNCoef];
-          load_coef(a.tabf, l * N + min(n + 1, N - 1), seg, nsegf, nx);
+          load_coef(a.tabf, l * N + min(n + 1, N - 1), seg, fstride, nx);
           float p, dp;
           horner7_d(cf, t, p, dp);
 #pragma unroll
           for (int k = 0; k < kNCoef; ++k) cf[k] = nx[k];
-          // an r = 0 edge adds nothing: its l = 0 term has no gradient and
-          // B_nl(0) = 0 for l >= 1, so b = 0 there (and h = 0 through dt_r)
-          const float b = self_edge ? 0.0f : p, h = dp * dt_r;
+          // xi sums G B, ze sums G dB/dt: the factor (dt/dr) / r of zeta is applied once, to Rz
           const float* gr = gs + n * KC + l * l;
 #pragma unroll
           for (int m = 0; m < 2 * l + 1; ++m) {
             const float gv = gr[m];
-            xi[m] = fmaf(gv, b, xi[m]);
-            ze[m] = fmaf(gv, h, ze[m]);
+            xi[m] = fmaf(gv, p, xi[m]);
+            ze[m] = fmaf(gv, dp, ze[m]);
           }
         }
         // this l's terms of the grouped sums (xi / ze index l + m within the l block)
@@ -481,6 +481,14 @@ __global__ void __launch_bounds__(128) k_forces(ForceArgs a) {
           }
         }
       }
+      // an r = 0 edge adds nothing: its l = 0 term has no gradient and B_nl(0) = 0 for l >= 1,
+      // so its xi terms are dropped here (and Rz through dt_r = 0)
+      const float keep = self_edge ? 0.0f : 1.0f;
+      P1 *= keep;
+      Pz *= keep;
+      Tx *= keep;
+      Ty *= keep;
+      Rz *= dt_r;
       const float rr = Rz - P1;
       const float ex = fmaf(x, rr, Tx), ey = fmaf(y, rr, Ty), ez = fmaf(z, Rz, Pz);
       if (!(a.attach && atom == catom)) {
@@ -567,7 +575,7 @@ struct ForceDispatch {
       if ((rc = check_launch("k_adjoint_g"))) return rc;
     }
     // edges
-    auto kern = (a.N == 8) ? k_forces<L, 8> : k_forces<L, 0>;
+    auto kern = (a.N == 8 && a.fstride == kForceSegStride) ? k_forces<L, true> : k_forces<L, false>;
     const int per_warp = 4 * ForceShape<L>::warp_floats(a.S, a.N);
     int wpb = (wpb_tuned == 1 || wpb_tuned == 2 || wpb_tuned == 4) ? wpb_tuned : 4;
     while (wpb > 1 && wpb * per_warp > 200 * 1024) wpb >>= 1;
@@ -641,6 +649,7 @@ extern "C" int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64
   a.N = b->n_max;
   a.S = b->n_species;
   a.nsegf = 2 * b->n_seg;
+  a.fstride = force_tab_stride(b->n_seg);
   a.F = b->n_feat_ps;
   a.attach = attach ? 1 : 0;
   a.crossover = b->crossover ? 1 : 0;

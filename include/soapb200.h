@@ -105,7 +105,8 @@ typedef struct soapb_basis {
   int32_t n_feat_cc; /* SG:909-910 */
   int64_t bytes;     /* device bytes the basis needs */
   int64_t off_alpha, off_beta, off_tab_b, off_tab_bh, off_ftab, off_widx, off_err;  /* byte offsets into dev */
-  int64_t off_tabf;  /* function-major table of w B_nl on half-width segments (2 n_seg): value and derivative */
+  int64_t off_tabf;  /* function-major table of w B_nl on half-width segments (2 n_seg of them, rows 64
+                        half segments apart when they fit, else 2 n_seg): value and derivative */
   int64_t off_self, off_poly;      /* self values (n_max (l_max+1) float); device copy of h_poly */
   void* dev;         /* set by soapb_basis_build */
 } soapb_basis;
