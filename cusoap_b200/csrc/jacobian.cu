@@ -55,6 +55,7 @@ struct JacArgs {
   int* counter;                  // work queue of the compute kernel
   int* ent_cnt;                  // (n_centres) entries per centre
   unsigned long long* ent;       // sorted entries, centre c at ent_mult * pair_off[c]
+  unsigned long long* ent_tmp;   // merge buffer of a centre with more than cap entries, same offsets
   unsigned int* bitmap;          // (n_centres * n_inc) nonzero-row bits
   int64_t n_centres, n_inc;
   int N, S, nseg, F, mode, attach, cap, eb, ent_mult;
@@ -76,10 +77,11 @@ struct JacShape {
   __host__ __device__ static int cs_floats(int N, int S) { return (S * N * KC + 3) & ~3; }
 };
 
-// Per-centre entries (all threads of the CTA): (row, edge) of the included
-// atoms collected and sorted by row in shared memory.  Returns the count.
-__device__ int centre_entries(const JacArgs& a, int64_t p0, int P, int catom, int crow, unsigned long long* keys,
-                              int* s_nent) {
+// The (row, edge) entries of the centre's included atoms, in any order: each is
+// handed to put(k, key) with k = 0, 1, ... from a block counter.  Returns the
+// count (all threads of the CTA; ends with a barrier).
+template <class Put>
+__device__ int gather_entries(const JacArgs& a, int64_t p0, int P, int catom, int crow, int* s_nent, Put put) {
   const int tid = threadIdx.x, nth = blockDim.x;
   if (tid == 0) *s_nent = 0;
   __syncthreads();
@@ -87,25 +89,16 @@ __device__ int centre_entries(const JacArgs& a, int64_t p0, int P, int catom, in
     const int atom = __float_as_int(a.pairs[p0 + e].w) & kAtomMask;
     if (a.attach && atom == catom) continue;  // centre and neighbour terms cancel
     const int row = a.inc_row[atom];
-    if (row >= 0) {
-      const int k = atomicAdd(s_nent, 1);
-      if (k < a.cap) keys[k] = ((unsigned long long)row << 32) | (unsigned)e;
-    }
-    if (crow >= 0) {
-      const int k = atomicAdd(s_nent, 1);
-      if (k < a.cap) keys[k] = ((unsigned long long)crow << 32) | (unsigned)e;
-    }
+    if (row >= 0) put(atomicAdd(s_nent, 1), ((unsigned long long)row << 32) | (unsigned)e);
+    if (crow >= 0) put(atomicAdd(s_nent, 1), ((unsigned long long)crow << 32) | (unsigned)e);
   }
   __syncthreads();
-  int nent = *s_nent;
-  if (nent > a.cap) {
-    if (tid == 0) atomicOr(a.status, 1);
-    nent = a.cap;
-  }
-  int n2 = 1;
-  while (n2 < nent) n2 <<= 1;
-  for (int i = nent + tid; i < n2; i += nth) keys[i] = ~0ull;
-  __syncthreads();
+  return *s_nent;
+}
+
+// Ascending bitonic sort of n2 (a power of two) keys in shared memory (all threads of the CTA).
+__device__ void block_bitonic(unsigned long long* keys, int n2) {
+  const int tid = threadIdx.x, nth = blockDim.x;
   for (int k = 2; k <= n2; k <<= 1)
     for (int j = k >> 1; j > 0; j >>= 1) {
       for (int i = tid; i < n2; i += nth) {
@@ -118,6 +111,77 @@ __device__ int centre_entries(const JacArgs& a, int64_t p0, int P, int catom, in
       }
       __syncthreads();
     }
+}
+
+// Sorts n keys (n <= cap) in shared memory, padding to a power of two with ~0.
+__device__ void sort_tile(unsigned long long* keys, int n) {
+  int n2 = 1;
+  while (n2 < n) n2 <<= 1;
+  for (int i = n + threadIdx.x; i < n2; i += blockDim.x) keys[i] = ~0ull;
+  __syncthreads();
+  block_bitonic(keys, n2);
+}
+
+// Merges the sorted runs A[0, na) and B[0, nb) (distinct keys) into O: thread t
+// writes a contiguous share of the outputs, starting where a binary search of
+// the merge path puts its first output (all threads of the CTA).
+__device__ void merge_runs(const unsigned long long* A, int na, const unsigned long long* B, int nb,
+                           unsigned long long* O) {
+  const int total = na + nb, nth = blockDim.x;
+  const int per = (total + nth - 1) / nth;
+  const int o0 = threadIdx.x * per, o1 = min(o0 + per, total);
+  if (o0 >= total) return;
+  int lo = max(0, o0 - nb), hi = min(o0, na);
+  while (lo < hi) {  // fewest outputs from A such that the next A key follows the last B key taken
+    const int i = (lo + hi) >> 1;
+    if (A[i] < B[o0 - i - 1]) lo = i + 1;
+    else hi = i;
+  }
+  int i = lo, j = o0 - lo;
+  for (int o = o0; o < o1; ++o) O[o] = (j >= nb || (i < na && A[i] < B[j])) ? A[i++] : B[j++];
+}
+
+// Per-centre entries sorted by row into dst (global memory).  Centres whose
+// entries fit the shared-memory buffer (cap keys) are gathered and sorted
+// there.  Larger centres are gathered straight into dst, sorted in tiles of
+// cap keys in shared memory, and the sorted runs merged pairwise through tmp
+// (the same slot in a second buffer) until one run is left.  Keys are
+// distinct, so the order is the same however the gather was interleaved.
+__device__ int centre_entries(const JacArgs& a, int64_t p0, int P, int catom, int crow, unsigned long long* skeys,
+                              unsigned long long* dst, unsigned long long* tmp, int* s_nent) {
+  const int tid = threadIdx.x, nth = blockDim.x;
+  if (a.ent_mult * P <= a.cap) {
+    const int nent = gather_entries(a, p0, P, catom, crow, s_nent,
+                                    [&](int k, unsigned long long key) { skeys[k] = key; });
+    sort_tile(skeys, nent);
+    for (int i = tid; i < nent; i += nth) dst[i] = skeys[i];
+    __syncthreads();
+    return nent;
+  }
+  const int nent = gather_entries(a, p0, P, catom, crow, s_nent,
+                                  [&](int k, unsigned long long key) { dst[k] = key; });
+  for (int t0 = 0; t0 < nent; t0 += a.cap) {
+    const int n = min(a.cap, nent - t0);
+    for (int i = tid; i < n; i += nth) skeys[i] = dst[t0 + i];
+    sort_tile(skeys, n);
+    for (int i = tid; i < n; i += nth) dst[t0 + i] = skeys[i];
+    __syncthreads();
+  }
+  unsigned long long *src = dst, *out = tmp;
+  for (int w = a.cap; w < nent; w *= 2) {
+    for (int lo = 0; lo < nent; lo += 2 * w) {
+      const int mid = min(lo + w, nent), hi = min(lo + 2 * w, nent);
+      merge_runs(src + lo, mid - lo, src + mid, hi - mid, out + lo);
+    }
+    __syncthreads();
+    unsigned long long* s = src;
+    src = out;
+    out = s;
+  }
+  if (src != dst) {
+    for (int i = tid; i < nent; i += nth) dst[i] = src[i];
+    __syncthreads();
+  }
   return nent;
 }
 
@@ -129,12 +193,11 @@ __global__ void __launch_bounds__(256) k_jac_entries(JacArgs a) {
     const int P = (int)(a.pair_off[c + 1] - p0);
     const int catom = a.attach ? a.centre_atom[c] : -1;
     const int crow = (catom >= 0) ? a.inc_row[catom] : -1;
-    const int nent = centre_entries(a, p0, P, catom, crow, skeys, &s_nent);
     unsigned long long* dst = a.ent + (size_t)a.ent_mult * p0;
+    unsigned long long* tmp = a.ent_tmp + (size_t)a.ent_mult * p0;
+    const int nent = centre_entries(a, p0, P, catom, crow, skeys, dst, tmp, &s_nent);
     for (int i = threadIdx.x; i < nent; i += blockDim.x) {
-      const unsigned long long key = skeys[i];
-      dst[i] = key;
-      const int64_t r = (int64_t)c * a.n_inc + (int64_t)(key >> 32);
+      const int64_t r = (int64_t)c * a.n_inc + (int64_t)(dst[i] >> 32);
       atomicOr(a.bitmap + (r >> 5), 1u << (r & 31));
     }
     if (threadIdx.x == 0) a.ent_cnt[c] = nent;
@@ -455,7 +518,7 @@ __global__ void __launch_bounds__(256) k_jacobian(JacArgs a) {
 // ---------------------------------------------------------------------------
 
 struct JacLayout {
-  int64_t counter, ent_cnt, ent, bitmap, total;
+  int64_t counter, ent_cnt, ent, ent_tmp, bitmap, total;
 };
 
 static JacLayout jac_layout(int64_t n_centres, int64_t n_pairs, int64_t n_inc, int attach) {
@@ -465,6 +528,7 @@ static JacLayout jac_layout(int64_t n_centres, int64_t n_pairs, int64_t n_inc, i
   L.counter = take(16);
   L.ent_cnt = take(4 * n_centres);
   L.ent = take(8 * (attach ? 2 : 1) * (n_pairs > 0 ? n_pairs : 1));
+  L.ent_tmp = take(8 * (attach ? 2 : 1) * (n_pairs > 0 ? n_pairs : 1));
   L.bitmap = take(4 * ((n_centres * n_inc + 31) / 32));
   L.total = off;
   return L;
@@ -546,10 +610,11 @@ extern "C" int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int
   const JacLayout Lw = jac_layout(n_centres, n_pairs, n_inc, attach);
   if (work_bytes < Lw.total) return set_error(SOAPB_ERR_ARG, "jacobian workspace too small (%lld < %lld)",
                                               (long long)work_bytes, (long long)Lw.total);
-  const int need = (attach ? 2 : 1) * (max_pairs > 0 ? max_pairs : 1);
+  // shared-memory sort buffer of the entries kernel: the largest centre's entries, at most 8192
+  // keys (64 KB); each centre with more entries takes the tiled merge in the workspace
+  const int64_t need = (int64_t)(attach ? 2 : 1) * (max_pairs > 0 ? max_pairs : 1);
   int cap = 64;
-  while (cap < need) cap <<= 1;
-  if (cap > 8192) return set_error(SOAPB_ERR_UNSUPPORTED, "%d pairs per centre exceed the jacobian kernel's 8192", need);
+  while (cap < need && cap < 8192) cap <<= 1;
   cudaStream_t st = (cudaStream_t)stream;
   char* w = (char*)d_work;
   JacArgs a;
@@ -567,6 +632,7 @@ extern "C" int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int
   a.counter = (int*)(w + Lw.counter);
   a.ent_cnt = (int*)(w + Lw.ent_cnt);
   a.ent = (unsigned long long*)(w + Lw.ent);
+  a.ent_tmp = (unsigned long long*)(w + Lw.ent_tmp);
   a.bitmap = (unsigned int*)(w + Lw.bitmap);
   a.n_centres = n_centres;
   a.n_inc = n_inc;

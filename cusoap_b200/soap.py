@@ -43,9 +43,10 @@ from .xyz import ATOMIC_NUMBERS as _SYMBOLS
 MAX_N_MAX, MAX_L_MAX, MAX_SPECIES = 16, 12, 16
 # l_max 10-12 are built for n_max up to 8 (two lanes per l, four radial functions per lane)
 MAX_N_MAX_HIGH_L = 8
-# Per-centre (row, edge) entries the closed-form Jacobian kernel stages
-# (csrc/jacobian.cu): one per neighbour pair, two with attach=True.
-JACOBIAN_MAX_ENTRIES = 8192
+# Per-centre (row, edge) entries (one per neighbour pair of an included atom,
+# two with attach=True) that the Jacobian sorts in shared memory in one tile;
+# centres with more are sorted in tiles and merged in the workspace.
+JACOBIAN_TILE_ENTRIES = 8192
 
 _F64_WARNED = False
 
@@ -880,8 +881,9 @@ class SOAP:
                     only_physical_cores: bool = False, verbose: bool = False):
         """(n_centres, n_atoms_included, 3, n_features) Jacobian, and the
         descriptor, returned as ``(deriv, desc)`` when return_descriptor
-        (SG:2628-2699).  "auto"/"analytical" use the closed-form kernel;
-        "numerical" uses central differences of create() (step 1e-4)."""
+        (SG:2628-2699).  "auto"/"analytical" use the closed-form kernel, for
+        any number of neighbours per centre; "numerical" uses central
+        differences of create() (step FD_STEP, 5e-3 A)."""
         if method == "numerical":
             return self.derivatives_numerical(system, centers, include, exclude, method="numerical",
                                               return_descriptor=return_descriptor, attach=attach, n_jobs=n_jobs,
@@ -899,12 +901,6 @@ class SOAP:
             mode = self._out_mode()
             F = self.get_number_of_features()
             pairs = _Pairs(self, batch, _lib.NL_ALL)
-            entries = (2 if attach else 1) * pairs.max_pairs
-            if entries > JACOBIAN_MAX_ENTRIES:
-                raise ValueError(f"derivatives: a centre has {pairs.max_pairs} neighbours within the cutoff "
-                                 f"({entries} Jacobian entries{' with attach=True' if attach else ''}); the "
-                                 f"closed-form Jacobian kernel stages at most {JACOBIAN_MAX_ENTRIES} per centre. "
-                                 f"Use a smaller r_cut or the adjoint (create() with positions requiring grad).")
             desc, coeff = self._run_descriptor(batch, pairs, mode, want_coeff=True)
             deriv = torch.empty((batch.n_centres, n_inc, 3, F), dtype=torch.float32, device=self.device)
             if n_inc > 0 and batch.n_centres > 0:
@@ -924,9 +920,9 @@ class SOAP:
                            _ptr(pairs.pair_off), _ptr(pairs.pairs), pairs.total, _ptr(coeff), _ptr(inc_row), n_inc,
                            _ptr(batch.centre_attach), int(bool(attach)), pairs.max_pairs, mode,
                            _ptr(deriv), _ptr(work), work.numel(), _ptr(status), _stream(self.device))
-                # The kernel's per-centre entry capacity comes from pairs.max_pairs, the exact
-                # largest pair count of this list, so its overflow flag cannot be set here and is
-                # not read back: the call returns without waiting for the Jacobian to finish.
+                # The status word is never set (a centre with more entries than the kernel's
+                # shared-memory sort holds is merged in the workspace), so it is not read back:
+                # the call returns without waiting for the Jacobian to finish.
             if self.dtype != torch.float32:
                 deriv, desc = deriv.to(self.dtype), desc.to(self.dtype)
             return (deriv, desc) if return_descriptor else deriv

@@ -224,8 +224,9 @@ int soapb_neighbors_noalloc(const soapb_basis* b, const soapb_structs* s, const 
 int soapb_descriptor(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
                      int32_t out_mode, float* d_out, float* d_coeff, int32_t* d_counter, void* stream);
 
-/* Workspace bytes of soapb_jacobian (sorted per-centre entries, a nonzero-row
- * bitmap, a work counter) for n_pairs = d_pair_off[n_centres] pairs. */
+/* Workspace bytes of soapb_jacobian (sorted per-centre entries and a merge
+ * buffer of the same size, a nonzero-row bitmap, a work counter) for
+ * n_pairs = d_pair_off[n_centres] pairs. */
 int soapb_jacobian_workspace(const soapb_basis* b, int64_t n_centres, int64_t n_pairs, int64_t n_inc,
                              int32_t attach, int64_t* bytes);
 /* Dense Jacobian of the descriptor w.r.t. the included atoms: d_out
@@ -234,12 +235,14 @@ int soapb_jacobian_workspace(const soapb_basis* b, int64_t n_centres, int64_t n_
  * d_coeff) on the same SOAPB_NL_ALL pairs.  d_inc_row: (n_atoms,) output row
  * of each atom or -1.  attach = 0: fixed centres (DScribe convention,
  * SG:2297-2301); 1: centres move with their atom (d_centre_atom), adding the
- * centre-motion term.  max_pairs: upper bound on the pairs of any centre.
- * out_mode PS or CC.  d_status: int32 flag, nonzero if a centre exceeded the
- * kernel's staging capacity (it cannot be set when max_pairs is a true upper
- * bound, e.g. the largest count from soapb_neighbors_stats).  Every edge of an atom accumulates, so periodic
- * images are handled.  Replaces derivatives_analytical_ps SG:2270-2626 and
- * its Triton kernels SG:50-220. */
+ * centre-motion term.  max_pairs: the largest pair count of any centre (e.g.
+ * from soapb_neighbors_stats); it sizes the shared-memory sort of a centre's
+ * entries (up to 8192).  A centre with more entries (pairs of included atoms,
+ * twice with attach) than that buffer holds is sorted in tiles and merged in
+ * the workspace, so there is no limit per centre.  out_mode PS or CC.
+ * d_status: int32 word, kept for the ABI and never set.  Every edge of an
+ * atom accumulates, so periodic images are handled.  Replaces
+ * derivatives_analytical_ps SG:2270-2626 and its Triton kernels SG:50-220. */
 int soapb_jacobian(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_off, const void* d_pairs,
                    int64_t n_pairs, const float* d_coeff, const int32_t* d_inc_row, int64_t n_inc,
                    const int32_t* d_centre_atom, int32_t attach, int32_t max_pairs, int32_t out_mode, float* d_out,

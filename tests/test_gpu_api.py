@@ -174,18 +174,29 @@ def test_forces_status_word_is_clear_after_an_adjoint():
     assert torch.isfinite(pos.grad).all()
 
 
-def test_jacobian_entry_limit_is_a_clear_error():
-    """More neighbours per centre than the closed-form Jacobian kernel stages
-    (JACOBIAN_MAX_ENTRIES; half that with attach=True) is refused before any
-    Jacobian work, naming the limit; the adjoint path has no such limit."""
+def test_jacobian_beyond_one_shared_memory_tile():
+    """A centre with more (row, edge) entries than the Jacobian sorts in one
+    shared-memory tile (JACOBIAN_TILE_ENTRIES) is sorted in tiles and merged:
+    8232 atoms all within the cutoff of centre 0 give 8232 entries (one
+    merge), 16462 with attach=True (two merge passes), and a 4-atom include
+    list takes the same path with a single tile.  Checked against the
+    oracle's fixed-centre Jacobian; with attach the centre atom's row is the
+    fixed row minus the sum of all fixed rows (translation invariance)."""
     from cusoap_b200 import SOAP
-    from cusoap_b200.soap import JACOBIAN_MAX_ENTRIES
-    sysd = W.water_cluster(14, 14, 14, seed=1)  # 8232 atoms, every one within the cutoff of atom 0
-    s = SOAP(species=[1, 8], r_cut=100.0, n_max=2, l_max=1, sigma=0.5)
-    with pytest.raises(ValueError, match=str(JACOBIAN_MAX_ENTRIES)):
-        s.derivatives(sysd, centers=[0], include=[0])
-    small = W.water_cluster(12, 12, 12, seed=1)  # 5184 atoms: fits without attach, not with it
-    J = s.derivatives(small, centers=[0], include=[0, 1], return_descriptor=False)
-    assert J.shape == (1, 2, 3, s.get_number_of_features()) and torch.isfinite(J).all()
-    with pytest.raises(ValueError, match="attach"):
-        s.derivatives(small, centers=[0], include=[0], attach=True)
+    from cusoap_b200.soap import JACOBIAN_TILE_ENTRIES
+    from oracle.soap_oracle import OracleSOAP
+    sysd = W.water_cluster(14, 14, 14, seed=1)  # 8232 atoms
+    A = len(sysd["atomic_numbers"])
+    assert A > JACOBIAN_TILE_ENTRIES
+    P = dict(species=[1, 8], r_cut=100.0, n_max=2, l_max=1, sigma=0.5)
+    s, o = SOAP(**P), OracleSOAP(**P)
+    Jo = o.derivatives(sysd["positions"], sysd["atomic_numbers"], centers=[0], return_descriptor=False)
+    J = s.derivatives(sysd, centers=[0], return_descriptor=False).cpu().numpy()
+    assert _block_err(J, Jo) < DERIV_TOL
+    Ja = s.derivatives(sysd, centers=[0], attach=True, return_descriptor=False).cpu().numpy()
+    Jao = Jo.copy()
+    Jao[0, 0] = Jo[0, 0] - Jo[0].sum(axis=0)
+    assert _block_err(Ja, Jao) < DERIV_TOL
+    few = [0, 1, 2, 100]
+    Jf = s.derivatives(sysd, centers=[0], include=few, return_descriptor=False).cpu().numpy()
+    assert _block_err(Jf, Jo[:, few]) < DERIV_TOL
