@@ -555,10 +555,13 @@ __device__ __forceinline__ void visit(const VisitArgs& A, int64_t c, Fn&& fn) {
 // form one candidate stream that all lanes walk 32 at a time: a lane finds
 // its run from the run starts inside its tile (one OR-reduction and a
 // popcount).  Candidate order: z rows, then y, then x, then atom index --
-// deterministic, like the full window's.
+// deterministic, like the full window's.  PIPE: the candidate records of the
+// next tile are looked up and loaded while this tile is tested (the fill,
+// whose per-candidate work covers the load; the count, which has little work
+// per candidate, runs more warps instead).
 constexpr int kRunsPerPass = 128;  // 32 rows x at most 4 runs
 
-template <class Fn>
+template <bool PIPE, class Fn>
 __device__ __forceinline__ void visit_fine(const VisitArgs& A, int64_t c, int* runs, Fn&& fn) {
   const int lane = threadIdx.x & 31;
   const double4 cp = A.cpos[c];
@@ -666,19 +669,44 @@ __device__ __forceinline__ void visit_fine(const VisitArgs& A, int64_t c, int* r
         }
     }
     __syncwarp();
-    int rb = -1;  // run of the position before the tile
-    for (int k0 = 0; k0 < total; k0 += 32) {
+    // the run of each lane's position in the tile at k0, given the run rb of the position
+    // before the tile; returns the run of the tile's last position
+    auto lookup = [&](int k0, int rb, int& run) {
       const int idx = rb + 1 + lane;
       const int pos = (idx < nruns) ? r_start[idx] - k0 : 32;
       const unsigned mask = __reduce_or_sync(0xffffffffu, (pos >= 0 && pos < 32) ? (1u << pos) : 0u);
-      const int run = rb + __popc(mask & ((2u << lane) - 1u));
-      rb = __shfl_sync(0xffffffffu, run, 31);
+      run = rb + __popc(mask & ((2u << lane) - 1u));
+      return __shfl_sync(0xffffffffu, run, 31);
+    };
+    auto load = [&](int k, int run) { return A.sorted_pos[(int64_t)r_s0[run] + (k - r_start[run])]; };
+    const double4 zero4 = make_double4(0.0, 0.0, 0.0, 0.0);
+    int rb = -1;  // run of the position before the tile
+    int run_n = 0;
+    double4 rec_n = zero4;
+    if constexpr (PIPE) {
+      rb = lookup(0, -1, run_n);
+      if (lane < total) rec_n = load(lane, run_n);
+    }
+    for (int k0 = 0; k0 < total; k0 += 32) {
       const int k = k0 + lane;
+      int run;
+      double4 p = zero4;
+      if constexpr (PIPE) {
+        run = run_n;
+        p = rec_n;
+        rec_n = zero4;
+        if (k0 + 32 < total) {
+          rb = lookup(k0 + 32, rb, run_n);
+          if (k + 32 < total) rec_n = load(k + 32, run_n);
+        }
+      } else {
+        rb = lookup(k0, rb, run);
+        if (k < total) p = load(k, run);
+      }
       bool ok = false;
       int atom = 0, sp = 0;
       double rx = 0.0, ry = 0.0, rz = 0.0, r2 = 0.0;
       if (k < total) {
-        const double4 p = A.sorted_pos[(int64_t)r_s0[run] + (k - r_start[run])];
         int wrap;
         unpack_info(p.w, atom, sp, wrap);
         if (!g.any_per) {  // open structure: no image shifts (warp-uniform)
@@ -713,13 +741,15 @@ __device__ __forceinline__ void visit_fine(const VisitArgs& A, int64_t c, int* r
 
 // The enumeration for the centre's structure: sphere-trimmed for diagonal
 // frames, the full window otherwise (runs: kRunsPerPass * 3 ints of the warp's shared memory).
-template <class Fn>
+template <bool PIPE = false, class Fn>
 __device__ __forceinline__ void visit_any(const VisitArgs& A, int64_t c, int* runs, Fn&& fn) {
-  if (A.grids[A.cinfo[c].y].orth) visit_fine(A, c, runs, fn);
+  if (A.grids[A.cinfo[c].y].orth) visit_fine<PIPE>(A, c, runs, fn);
   else visit(A, c, fn);
 }
 
-__global__ void __launch_bounds__(128) k_count(VisitArgs A, int64_t n_centres, int* counts) {
+// 8 blocks of 4 warps per SM (64 registers): the count is latency-bound with
+// little work per candidate, so more resident warps pay more than pipelining.
+__global__ void __launch_bounds__(128, 8) k_count(VisitArgs A, int64_t n_centres, int* counts) {
   __shared__ int s_runs[4][3 * kRunsPerPass];
   const int lane = threadIdx.x & 31;
   const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
@@ -789,7 +819,7 @@ __global__ void __launch_bounds__(128) k_fill(VisitArgs A, int64_t n_centres, co
     __syncwarp();
     if (P <= kFillStage) {
       int n = 0;
-      visit_any(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double) {
+      visit_any<true>(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double) {
         const unsigned bal = __ballot_sync(0xffffffffu, ok);
         if (ok) {
           const int pos = n + __popc(bal & ((1u << lane) - 1u));
@@ -820,12 +850,12 @@ __global__ void __launch_bounds__(128) k_fill(VisitArgs A, int64_t n_centres, co
         __syncwarp();
       }
     } else {
-      visit_any(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double) {
+      visit_any<true>(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double) {
         if (ok) atomicAdd(&hist[keyof(record(atom, sp, rx, ry, rz))], 1);
       });
       __syncwarp();
       scan_hist();
-      visit_any(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double) {
+      visit_any<true>(A, c, runs, [&](bool ok, int atom, int sp, double rx, double ry, double rz, double) {
         const float4 rec = record(atom, sp, rx, ry, rz);
         const int key = ok ? keyof(rec) : -1 - lane;
         const unsigned peers = __match_any_sync(0xffffffffu, key);
