@@ -288,14 +288,31 @@ def test_cluster3000_create_and_derivatives():
 
 
 def test_cells512_batched():
+    """The batched create of all 512 cells against the oracle: every centre of 12 cells (the
+    smallest, the largest and 10 drawn with a fixed seed); then the batched adjoint forces of
+    E = sum w.p over 3 of them (one create_flat launch per stage, one backward)."""
     cells = W.make("cells512")
     s = _soap("cells512")
     out = s.create(cells)
     o = _oracle("cells512")
-    for k in (0, 100, 511):
+    sizes = [len(c["atomic_numbers"]) for c in cells]
+    rng = np.random.default_rng(7)
+    pick = sorted({int(np.argmin(sizes)), int(np.argmax(sizes))} |
+                  {int(k) for k in rng.choice(len(cells), 10, replace=False)})
+    for k in pick:
         c = cells[k]
-        ref = o.create(c["positions"], c["atomic_numbers"], centers=[0, 1, 2], cell=c["cell"], pbc=c["pbc"])
-        assert _row_err(_np(out[k][:3]), ref) < DESC_TOL
+        ref = o.create(c["positions"], c["atomic_numbers"], cell=c["cell"], pbc=c["pbc"])
+        assert _row_err(_np(out[k]), ref) < DESC_TOL, k
+    sub = [cells[k] for k in sorted({pick[len(pick) // 2], int(np.argmin(sizes)), int(np.argmax(sizes))})]
+    w = rng.standard_normal(s.get_number_of_features())
+    wt = torch.tensor(w, dtype=torch.float32, device="cuda")
+    pos = [torch.tensor(c["positions"], device="cuda", requires_grad=True) for c in sub]
+    flat, _ = s.create_flat([dict(c, positions=p) for c, p in zip(sub, pos)])
+    (flat @ wt).sum().backward()
+    for c, p in zip(sub, pos):
+        Fo = o.forces(c["positions"], c["atomic_numbers"], np.tile(w, (len(c["atomic_numbers"]), 1)),
+                      cell=c["cell"], pbc=c["pbc"])
+        assert rel_l2(-_np(p.grad), Fo) < DERIV_TOL
 
 
 def test_waterbox2001_forces_vs_oracle():
