@@ -23,7 +23,8 @@ EXPORTS = (
     "soapb_neighbors_workspace", "soapb_neighbors_count", "soapb_neighbors_fill", "soapb_neighbors_status",
     "soapb_neighbors_stats", "soapb_neighbors_clamp", "soapb_neighbors_noalloc",
     "soapb_descriptor", "soapb_jacobian_workspace", "soapb_jacobian", "soapb_forces_workspace", "soapb_forces",
-    "soapb_forces_status", "soapb_last_error", "soapb_version", "soapb_kernel_launches",
+    "soapb_forces_status", "soapb_check_bounded_wait", "soapb_last_error", "soapb_version",
+    "soapb_kernel_launches",
 )
 
 
@@ -95,6 +96,7 @@ def load() -> ctypes.CDLL:
         "soapb_forces_workspace": [POINTER(Basis), c_int64, POINTER(c_int64)],
         "soapb_forces": [POINTER(Basis), c_int64, P, P, P, P, c_int32, P, c_int32, P, P, c_int64, P, P],
         "soapb_forces_status": [POINTER(Basis), c_int64, P, POINTER(c_int32), P],
+        "soapb_check_bounded_wait": [P, P],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

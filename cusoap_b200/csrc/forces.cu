@@ -674,3 +674,27 @@ extern "C" int soapb_forces_status(const soapb_basis* b, int64_t n_centres, cons
   if (rc) return rc;
   return check_cuda(cudaStreamSynchronize(st), "forces status sync");
 }
+
+namespace soapb {
+
+// Diagnostic of the G stage's bounded wait: one thread arms an mbarrier with a
+// transaction count that no copy will fill and waits on it as the G stage
+// waits for its row copies.  The wait gives up after about one second and the
+// thread writes 1 to *status (0 would mean the phase completed).  No copy is
+// in flight, so nothing can land after the block exits.
+__global__ void k_check_bounded_wait(int* status) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  mbar_expect_tx(&bar, 16);
+  *status = mbar_wait(&bar, 0) ? 0 : 1;
+}
+
+}  // namespace soapb
+
+extern "C" int soapb_check_bounded_wait(int32_t* d_status, void* stream) {
+  if (!d_status) return set_error(SOAPB_ERR_ARG, "null status");
+  k_check_bounded_wait<<<1, 32, 0, (cudaStream_t)stream>>>(d_status);
+  return check_launch("k_check_bounded_wait");
+}

@@ -273,6 +273,12 @@ int soapb_forces(const soapb_basis* b, int64_t n_centres, const int64_t* d_pair_
  * counterpart in the reference (autograd reports no device status). */
 int soapb_forces_status(const soapb_basis* b, int64_t n_centres, const void* d_work, int32_t* h_status,
                         void* stream);
+/* Diagnostic of the failure path above: one block waits, with the G stage's
+ * bounded wait, on a barrier that no copy completes, gives up after about one
+ * second and writes 1 to the device int32 *d_status (0 if the wait had ended
+ * normally).  Stream-ordered; no copy is in flight, so the context stays
+ * usable.  No counterpart in the reference. */
+int soapb_check_bounded_wait(int32_t* d_status, void* stream);
 
 /* Message describing the last error on the calling thread ("" if none). */
 const char* soapb_last_error(void);

@@ -174,6 +174,29 @@ def test_forces_status_word_is_clear_after_an_adjoint():
     assert torch.isfinite(pos.grad).all()
 
 
+def test_bounded_wait_gives_up_and_the_context_stays_usable(golden):
+    """The bounded wait behind the adjoint's row copies ends on its own: a block
+    waits on a barrier that no copy completes, gives up after about a second and
+    reports status 1; the same context then still computes the reference's
+    descriptors."""
+    import ctypes
+    import time
+    from cusoap_b200 import _lib
+    lib = _lib.load()
+    status = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _lib.check(lib.soapb_check_bounded_wait(ctypes.c_void_p(status.data_ptr()),
+                                            ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    waited = time.perf_counter() - t0
+    assert int(status.item()) == 1
+    assert 0.5 < waited < 30.0
+    g = golden("cluster192")
+    d = _soap("cluster192").create({"positions": g["positions"], "atomic_numbers": g["Z"]})
+    assert _block_err(d.cpu().numpy(), g["create_off"]) < 1e-5
+
+
 def test_jacobian_beyond_one_shared_memory_tile():
     """A centre with more (row, edge) entries than the Jacobian sorts in one
     shared-memory tile (JACOBIAN_TILE_ENTRIES) is sorted in tiles and merged:
