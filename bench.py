@@ -522,6 +522,14 @@ def diff_forces(soap_cls, torch, steps: int = 20, warmup: int = 3):
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 148 SMs x 128 FP32 lanes x FMA at the 1965 MHz max clock
 
 
+def harmonics_flop(L: int) -> int:
+    """FLOP of one pair's real solid harmonics up to l_max = L, as the kernels
+    compute them: r^2 (5); the Legendre table Q_l^m -- L entries Q_{m+1}^m at 1
+    FLOP and (L-1)L/2 three-term entries at 5; the powers (x + i y)^m, 6 per m;
+    the (L+1)(L+2)/2 normalisations and the L(L+1) products with cos/sin."""
+    return 5 + L + 5 * (L - 1) * L // 2 + 6 * L + (L + 1) * (L + 2) // 2 + L * (L + 1)
+
+
 def scale_create(soap_cls, torch, steps: int = 3, warmup: int = 2, n_mol: int = 0):
     """The scale workload: create() on the 1,000,002-atom water cluster
     (n_max 8, l_max 4, F = 680, 2.72 GB of output), positions resident on the
@@ -555,7 +563,7 @@ def scale_create(soap_cls, torch, steps: int = 3, warmup: int = 2, n_mol: int = 
     N, L = W.CONFIGS["cluster1M"]["n_max"], W.CONFIGS["cluster1M"]["l_max"]
     K = (L + 1) ** 2
     # a degree-7 Horner pass is 7 FMAs = 14 FLOP per radial function and pair
-    flop = n_pairs * (2 * N * K + N * (L + 1) * 14) + n_at * 2 * F * K / (L + 1)
+    flop = n_pairs * (2 * N * K + N * (L + 1) * 14 + harmonics_flop(L)) + n_at * 2 * F * K / (L + 1)
     byts = n_pairs * 16 + n_at * F * 4
     d_ms = st.get("descriptor", float("nan"))
     peak, _ = _peaks()
@@ -566,8 +574,9 @@ def scale_create(soap_cls, torch, steps: int = 3, warmup: int = 2, n_mol: int = 
             "descriptor": {"hbm_bytes": byts, "gbs": byts / d_ms / 1e6, "hbm_frac_of_measured": byts / d_ms / 1e6 / peak,
                            "flop": flop, "tflops": flop / d_ms / 1e9,
                            "fp32_frac_of_nominal": flop / d_ms / 1e9 / FP32_PEAK_TFLOPS,
-                           "note": "flop = pairs x (2 N K accumulate + 14 N (l_max+1) radial Horner, 7 FMAs per function) + centres x "
-                                   "2 F K/(l_max+1) power spectrum; bytes = 16 B per pair read + F x 4 B per row"}}
+                           "note": "flop = pairs x (2 N K accumulate + 14 N (l_max+1) radial Horner, 7 FMAs per function + "
+                                   f"{harmonics_flop(L)} solid harmonics) + centres x 2 F K/(l_max+1) power spectrum; "
+                                   "bytes = 16 B per pair read + F x 4 B per row"}}
 
 
 def run_ours(args):
